@@ -1,0 +1,174 @@
+/*
+ * pot3d_gpu.h -- C-ABI of libpot3d_gpu.so, the B200 (sm_100a) PCG hot path
+ * of POT3D.
+ *
+ * Two groups of entry points:
+ *
+ * 1. The three legacy symbols of POT3D's external LU solver
+ *    (module external_lu_solver_interface, src/pot3d.F90:581-609), with the
+ *    same signatures and semantics as src/lusol_cusparse.c:64,309,374, so a
+ *    -DCUSPARSE build of the Fortran host links against this library instead
+ *    of the cuSPARSE shim.  Like the shim they take DEVICE pointers, keep a
+ *    single global instance, print "ERROR! ..." and exit(1) on failure.
+ *
+ * 2. pot3d_gpu_* : a whole-solve offload that replaces the body of
+ *    cgsolve (src/pot3d.F90:4231-4369) and the pieces of potfld around it
+ *    (RHS, phi finalisation, energies).  They return a status code
+ *    (POT3D_OK = 0) and never exit; pot3d_gpu_last_error() describes the
+ *    most recent failure on the calling thread.
+ *
+ * Layout conventions follow the reference exactly:
+ *  - 1-D mesh arrays are the local_mesh arrays of one rank (Fortran element
+ *    k is C element k-1): r,dr (nr-1); rh,drh (nr); t,dt,st (nt-1);
+ *    th,dth,sth (nt); p,dp,ph,dph (np).
+ *  - CG vectors are the packed interior vectors of potfld, length
+ *    N = (nr-2)*(nt-2)*(np-2), index (k-2)*(nt-2)*(nr-2)+(j-2)*(nr-2)+(i-2)
+ *    (src/pot3d.F90:3917,4930).
+ *  - 2-D/3-D fields (br0, phi) are Fortran column-major: br0(nt,np),
+ *    phi(nr,nt,np).
+ */
+#ifndef POT3D_GPU_H
+#define POT3D_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Legacy external LU solver (drop-in for src/lusol_cusparse.c)            */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces load_external_lu_solver, src/lusol_cusparse.c:64-302
+ * (Fortran interface src/pot3d.F90:587-593).  CSR_LU/CSR_I/CSR_J are DEVICE
+ * pointers to the 1-based CSR built by diacsr (src/pot3d.F90:4870-5018);
+ * N rows, M = CSR_I[N] as returned by getM.  Factorises CSR_LU in place into
+ * ILU(0) L\U (unit lower L, upper U), FP32, with the row operations of ilu0
+ * (src/pot3d.F90:4717-4813).  Keeps the pointers for external_lu_solver. */
+void load_external_lu_solver(float *CSR_LU, int *CSR_I, int *CSR_J, int N, int M);
+
+/* Replaces external_lu_solver, src/lusol_cusparse.c:309-367
+ * (src/pot3d.F90:595-600).  In place on the DEVICE FP64 vector x of length
+ * N: x <- (double)(U^-1 L^-1 (float)x), the sweeps of lusol
+ * (src/pot3d.F90:5227-5302) in FP32. */
+void external_lu_solver(double *x);
+
+/* Replaces unload_external_lu_solver, src/lusol_cusparse.c:374-391
+ * (src/pot3d.F90:602-604).  Frees what load_external_lu_solver allocated. */
+void unload_external_lu_solver(void);
+
+/* ---------------------------------------------------------------------- */
+/* Whole-solve offload                                                    */
+/* ---------------------------------------------------------------------- */
+
+enum {
+  POT3D_OK = 0,
+  POT3D_ERR_ARG = 1,        /* invalid argument or size */
+  POT3D_ERR_CUDA = 2,       /* CUDA runtime failure */
+  POT3D_ERR_NOMEM = 3,      /* device allocation failed */
+  POT3D_ERR_PIVOT = 4,      /* zero pivot in the ILU(0) factorisation */
+  POT3D_ERR_NOT_CONVERGED = 5,
+  POT3D_ERR_TIMEOUT = 6,    /* a bounded device wait ran out */
+  POT3D_ERR_BREAKDOWN = 7   /* non-finite or zero curvature in PCG */
+};
+
+/* Preconditioner choice, as the namelist's ifprec (src/pot3d.F90:428). */
+enum { POT3D_PREC_NONE = 0, POT3D_PREC_DIAG = 1, POT3D_PREC_ILU0 = 2 };
+
+/* Arithmetic of the solve. */
+enum {
+  POT3D_FP64 = 0,          /* the reference's classical FP64 PCG */
+  POT3D_FP32_REFINED = 1   /* FP32 stencil/preconditioner inner iterations
+                              inside an FP64 iterative-refinement loop */
+};
+
+typedef struct {
+  int nr, nt, np;
+  const double *r, *dr;           /* nr-1 */
+  const double *rh, *drh;         /* nr   */
+  const double *t, *dt, *st;      /* nt-1 */
+  const double *th, *dth, *sth;   /* nt   */
+  const double *p, *dp;           /* np   */
+  const double *ph, *dph;         /* np   */
+} pot3d_mesh_t;
+
+typedef struct pot3d_gpu_solver pot3d_gpu_solver;
+
+typedef struct {
+  int ncg;           /* iterations (FP64 PCG) or total inner iterations */
+  int n_refine;      /* FP64 residual replacements (refined mode) */
+  double epsn;       /* final epsn as ernorm defines it (src/pot3d.F90:4432) */
+  double true_resid; /* ||b - A x||_2 / ||b||_2 of the returned x, FP64 */
+  double seconds;    /* device time of the iteration (CUDA events) */
+  long long kernel_launches; /* kernels this library launched for the solve */
+} pot3d_solve_info_t;
+
+/* Set up a solve: copies the mesh and br0 (host pointers) to the device,
+ * forms the matrix-free operator of load_matrix_pot3d_solve
+ * (src/pot3d.F90:4565-4613) and the preconditioner of
+ * load_preconditioner_pot3d_solve (src/pot3d.F90:4615-4715).  pm_r1 is the
+ * r=R1 switch of check_input (src/pot3d.F90:1250-1285).  br1 may be NULL; if
+ * given, the validation-run Neumann condition at r=R1 is used
+ * (src/pot3d.F90:5420-5423).  device < 0 means the current device. */
+int pot3d_gpu_create(const pot3d_mesh_t *mesh, const double *br0, const double *br1,
+                     double pm_r1, int ifprec, int precision, int device,
+                     pot3d_gpu_solver **out);
+int pot3d_gpu_destroy(pot3d_gpu_solver *s);
+
+/* Number of unknowns N. */
+long pot3d_gpu_size(const pot3d_gpu_solver *s);
+
+/* RHS by potfld's boundary trick, src/pot3d.F90:3937-3950 (host output). */
+int pot3d_gpu_rhs(pot3d_gpu_solver *s, double *rhs);
+
+/* cgsolve(x, r, N, ierr), src/pot3d.F90:4231-4369, host pointers.  On entry
+ * x is the guess and r the RHS; on exit x is the solution and r the
+ * residual.  *ierr = 0 converged, 1 ncgmax exceeded (as the reference).
+ * info may be NULL. */
+int pot3d_gpu_cgsolve(pot3d_gpu_solver *s, double *x, double *r, long N, int ncgmax,
+                      double epscg, int *ierr, pot3d_solve_info_t *info);
+/* Same with DEVICE pointers (the Fortran host's use_device_addr arrays). */
+int pot3d_gpu_cgsolve_dev(pot3d_gpu_solver *s, double *x, double *r, long N, int ncgmax,
+                          double epscg, int *ierr, pot3d_solve_info_t *info);
+
+/* Residual history of the last solve: epsn after iterations 0..n-1
+ * (ernorm's value, src/pot3d.F90:4432-4433).  Returns how many were
+ * written (at most cap). */
+int pot3d_gpu_history(const pot3d_gpu_solver *s, double *eps, int cap);
+
+/* unpack_scalar + set_boundary_points(phi,1) + seam_hhh, the phi
+ * finalisation of potfld (src/pot3d.F90:3966-3969).  x: host, N.
+ * phi: host, (nr,nt,np) column-major. */
+int pot3d_gpu_finalize_phi(pot3d_gpu_solver *s, const double *x, double *phi);
+
+/* getb + magnetic_energy (src/pot3d.F90:6187-6321) from a host phi with
+ * ghosts; w = {W_r, W_t, W_p}. */
+int pot3d_gpu_energy(pot3d_gpu_solver *s, const double *phi, double w[3]);
+
+/* Kernel-level entry points for parity checks, DEVICE pointers, length N.
+ * ax: y = A x as ax (src/pot3d.F90:5102-5150), homogeneous boundaries.
+ * prec: x <- M^-1 x as prec_inv (src/pot3d.F90:5152-5225). */
+int pot3d_gpu_ax_dev(pot3d_gpu_solver *s, const double *x, double *y);
+int pot3d_gpu_prec_dev(pot3d_gpu_solver *s, double *x);
+/* The FP32 diagonal preconditioner a_i (src/pot3d.F90:4653-4661) or, for
+ * ifprec=2, the FP32 U diagonal of ILU(0) and its inverse a_csr_d
+ * (src/pot3d.F90:4706-4708); host outputs of length N (dinv may be NULL). */
+int pot3d_gpu_precond_diag(pot3d_gpu_solver *s, float *d, float *dinv);
+
+/* Times the two kernels of one FP64 PCG iteration with CUDA events on the
+ * solver's stream: reps iterations from a fresh start (r = b, p = 0), the
+ * stencil+dot kernel and the update+dot kernel timed separately.
+ * ms[0], ms[1] = average milliseconds per launch; bytes[0], bytes[1] = the
+ * algorithmic DRAM bytes per launch (stencil: r, p read, p, Ap written;
+ * update: x, p, r, Ap read, x, r written; 8 B each per unknown). */
+int pot3d_gpu_time_kernels(pot3d_gpu_solver *s, int reps, double ms[2], double bytes[2]);
+
+/* Message for the most recent failing call on this thread. */
+const char *pot3d_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POT3D_GPU_H */

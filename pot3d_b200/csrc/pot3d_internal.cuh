@@ -1,0 +1,117 @@
+// Internal definitions shared by the pot3d_gpu CUDA sources.
+//
+// Data layout in HBM: every CG vector lives in a padded interior layout
+//   idx = (kk * ntm2 + jj) * NRP + e
+// with e = i-2, jj = j-2, kk = k-2 the interior offsets of Fortran (i,j,k)
+// and NRP = nrm2 rounded up to a multiple of 16 doubles (128 B), so every
+// radial line starts on a 128-byte boundary and the double2/float2 loads of
+// the kernels are aligned.  Pad lanes hold zeros and are never written with
+// anything else.  The reference's packed layout (src/pot3d.F90:4930) is the
+// same with NRP = nrm2; pack/unpack kernels convert at the API boundary.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/pot3d_gpu.h"
+
+namespace pot3d {
+
+constexpr int TI = 64;      // radial points per tile (32 lanes x 2)
+constexpr int TJ = 8;       // theta rows per tile (one warp each)
+constexpr int NTHR = 256;   // threads per tile block
+constexpr int SROW = TI + 4;  // shared-memory row: [pad, halo-, 64 own, halo+, pad]
+
+// Mesh arrays on the device, 1-based Fortran indexing: arr[k] is Fortran
+// element k (one spare slot at 0 and at the end).
+struct DevMesh {
+  const double *drh, *dth, *sth_i, *dp_i, *dph, *st, *dt_i, *sth, *r2, *dr_i;
+  const double *dr, *rh, *dt, *dp;
+  const double *br0, *br1;  // (nt,np) column-major, 0-based
+  double dr1, drn, pm_r1, pl_i;
+};
+
+struct Geo {
+  int nr, nt, np;
+  int nrm2, ntm2, npm2;
+  int NRP;      // padded radial line length
+  int tk;       // k-planes per block in tiled kernels
+  int nkc;      // number of k chunks (gridDim.z)
+  int nit;      // number of i tiles (gridDim.x)
+  int njt;      // number of j tiles (gridDim.y)
+  long long Np; // padded vector length
+  long long N;  // packed vector length
+  __host__ __device__ long long idx(int e, int jj, int kk) const {
+    return ((long long)kk * ntm2 + jj) * NRP + e;
+  }
+};
+
+// Scalars of one PCG solve, resident on the device so the iteration never
+// waits on the host.
+struct SolveState {
+  double rho, rho_old, alpha, beta, bdotb, epsn, pq, epscg;
+  double rho_true;  // refined mode: preconditioned FP64 residual norm^2
+  int ncg, ncgmax, status, par;
+  unsigned int cnt_a, cnt_b, cnt_c, pad0;
+  int hist_cap, n_refine, inner, pad1;
+  double *hist;
+};
+
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXIT = 2, ST_BREAKDOWN = 3 };
+
+// ---- deterministic block reduction --------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the block in a fixed order; result valid in thread 0.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NT / 32; q++) s += sh[q];
+  }
+  return s;
+}
+
+// Last-block pattern: every block stores its partial, the block that
+// arrives last sums all partials in index order (deterministic for a fixed
+// grid) and returns true in all its threads with the total in *total.
+template <int NT>
+__device__ bool last_block_sum(double part, double *partials, unsigned int *counter,
+                               unsigned int nblocks, double *total, double *sh) {
+  __shared__ bool is_last;
+  const unsigned int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (threadIdx.x == 0) {
+    partials[b] = part;
+    __threadfence();
+    unsigned int prev = atomicAdd(counter, 1u);
+    is_last = (prev == nblocks - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  double s = 0.0;
+  for (unsigned int q = threadIdx.x; q < nblocks; q += NT) s += __ldcg(partials + q);
+  s = block_sum<NT>(s, sh);
+  if (threadIdx.x == 0) {
+    *total = s;
+    *counter = 0u;
+  }
+  return true;
+}
+
+}  // namespace pot3d
+
+// Error reporting shared by the C-ABI entry points.
+void pot3d_set_error(const std::string &msg);
+int pot3d_cuda_status(cudaError_t e, const char *where);

@@ -1,0 +1,88 @@
+// Host-side solver object behind the pot3d_gpu_* C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "pot3d_internal.cuh"
+
+namespace pot3d {
+
+struct DiluState;   // ILU(0) preconditioner (dilu.cu)
+struct MixedState;  // FP32-inner / FP64-refinement state (mixed.cu)
+
+struct Solver {
+  Geo g{};
+  DevMesh m{};
+  int ifprec = 1, precision = 0;
+  double pm_r1 = -1.0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<void *> allocs;
+
+  SolveState *d_state = nullptr;
+  SolveState *h_state = nullptr;
+  double *d_partials = nullptr;
+  size_t nblk_tiled = 0;
+  double *d_s1z = nullptr, *d_s1p = nullptr, *d_s1 = nullptr;
+  double *d_scalar = nullptr, *d_sums = nullptr, *d_hist = nullptr;
+  int hist_cap = 0;
+  // padded FP64 vectors
+  double *d_x = nullptr, *d_r = nullptr, *d_p = nullptr, *d_p2 = nullptr, *d_q = nullptr, *d_b = nullptr;
+  double *d_tmp = nullptr;      // scratch (API packing, residual)
+  double *d_ref = nullptr;      // scratch in the reference packed layout (N)
+  double *d_phi = nullptr;      // (nr,nt,np) scratch for finalize/energy
+  float *d_ai = nullptr;        // diagonal preconditioner (FP32, padded)
+  double *p_cur = nullptr, *p_nxt = nullptr;
+
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_U = 0, graph_kind = -1;
+
+  long long launches = 0;  // kernel launches of the last solve
+  int last_ncg = 0, last_refine = 0;
+  double last_epsn = 0.0, last_seconds = 0.0;
+
+  DiluState *dilu = nullptr;
+  MixedState *mixed = nullptr;
+
+  ~Solver();
+  int alloc(void **p, size_t bytes);
+  int setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1, double pm_r1, int ifprec,
+            int precision);
+  int pack(const double *ref_dev, double *pad_dev);
+  int unpack(const double *pad_dev, double *ref_dev);
+  int ax_padded(const double *x, double *y);
+  int prec_padded(double *x);  // x <- M^-1 x
+  int rhs_padded(double *b);
+  int dot_padded(const double *x, const double *y, double *out_dev);
+  int launch_iteration();
+  // FP64 PCG on d_x (guess) / d_b (RHS).  d_r holds the residual on exit.
+  int cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info);
+  int true_residual(double *out);  // ||b - A x|| / ||b|| of d_x, d_b
+  int finalize_phi_dev(const double *xpad, double *phi_dev);
+  int time_kernels(int reps, double ms[2], double bytes[2]);
+  int sweep_launches() const;  // kernels per ILU(0) application
+  int energy_dev(const double *phi_dev, double w[3]);
+};
+
+// ILU(0) preconditioner hooks (dilu.cu).
+int dilu_setup(Solver *s);
+void dilu_destroy(Solver *s);
+float *dilu_r32(Solver *s);   // FP32 input of the sweeps (padded layout)
+float *dilu_z32(Solver *s);   // FP32 output z = (LU)^-1 r32
+// Forward + backward sweeps r32 -> z32 on s->stream; with check_status the
+// kernels return at once when the PCG state is no longer running.
+int dilu_sweeps(Solver *s, bool check_status);
+int dilu_diag(Solver *s, float *d_host, float *dinv_host);
+int dilu_sweep_launches(Solver *s);
+
+// FP32-refined solve hooks (mixed.cu).
+int mixed_setup(Solver *s);
+void mixed_destroy(Solver *s);
+int mixed_solve(Solver *s, bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info);
+
+// Kernel launch helpers shared between translation units.
+int grid1d(long long n);
+
+}  // namespace pot3d

@@ -1,0 +1,155 @@
+"""Python mirror of POT3D's solve interface over the C-ABI.
+
+``Pot3dSolver`` holds one set-up solve (potfld's matrix and preconditioner
+load, src/pot3d.F90:3907-3935) on the GPU; ``cgsolve`` keeps the reference
+contract of cgsolve(x, r, N, ierr) (src/pot3d.F90:4231-4369): x is the
+guess on entry and the solution on exit, r the RHS on entry and the residual
+on exit, and ierr is 0 when converged and 1 when ncgmax was exceeded.
+``potfld`` runs the whole reference sequence: RHS by the boundary trick,
+PCG, phi with ghosts, and the magnetic energies of magnetic_energy.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import SolveInfo, check, dptr, fptr
+from .host import PM_R1, Mesh
+
+PRECISION = {"fp64": 0, "fp32_refined": 1}
+
+
+class Pot3dSolver:
+    def __init__(self, mesh: Mesh, br0, option: str = "ss", ifprec: int = 1, precision: str = "fp64",
+                 br1=None, device: int = -1):
+        self.mesh = mesh
+        self.option = option
+        self.ifprec = ifprec
+        self.precision = precision
+        self._br0 = np.asfortranarray(br0, dtype=np.float64)
+        self._br1 = None if br1 is None else np.asfortranarray(br1, dtype=np.float64)
+        self._mc = mesh.cstruct()
+        h = C.c_void_p()
+        check(_lib.lib().pot3d_gpu_create(C.byref(self._mc), dptr(self._br0),
+                                          None if self._br1 is None else dptr(self._br1), PM_R1[option], ifprec,
+                                          PRECISION[precision], device, C.byref(h)))
+        self._h = h
+        self.N = int(_lib.lib().pot3d_gpu_size(h))
+        self.last_info = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().pot3d_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- reference-shaped API ------------------------------------------
+    def rhs(self) -> np.ndarray:
+        b = np.zeros(self.N)
+        check(_lib.lib().pot3d_gpu_rhs(self._h, dptr(b)))
+        return b
+
+    def cgsolve(self, x: np.ndarray, r: np.ndarray, ncgmax: int = 10_000_000, epscg: float = 1e-9) -> int:
+        """In place on host arrays x (guess -> solution), r (RHS -> residual)."""
+        for a in (x, r):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != self.N:
+                raise ValueError("x and r must be contiguous float64 arrays of length N")
+        ierr = C.c_int(1)
+        info = SolveInfo()
+        check(_lib.lib().pot3d_gpu_cgsolve(self._h, dptr(x), dptr(r), self.N, ncgmax, epscg, C.byref(ierr),
+                                           C.byref(info)))
+        self.last_info = info
+        return ierr.value
+
+    def cgsolve_dev(self, x, r, ncgmax: int = 10_000_000, epscg: float = 1e-9) -> int:
+        """Same on CUDA tensors (device pointers), as the Fortran host's
+        use_device_addr arrays."""
+        for a in (x, r):
+            if not a.is_cuda or a.dtype.itemsize != 8 or not a.is_contiguous() or a.numel() != self.N:
+                raise ValueError("x and r must be contiguous float64 CUDA tensors of length N")
+        ierr = C.c_int(1)
+        info = SolveInfo()
+        check(_lib.lib().pot3d_gpu_cgsolve_dev(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(r.data_ptr()),
+                                               self.N, ncgmax, epscg, C.byref(ierr), C.byref(info)))
+        self.last_info = info
+        return ierr.value
+
+    def history(self, cap: int = 1 << 20) -> np.ndarray:
+        """epsn after iterations 0..ncg of the last solve."""
+        buf = np.zeros(cap)
+        n = _lib.lib().pot3d_gpu_history(self._h, dptr(buf), cap)
+        return buf[:n].copy()
+
+    def finalize_phi(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        phi = np.zeros((self.mesh.nr, self.mesh.nt, self.mesh.np), order="F")
+        check(_lib.lib().pot3d_gpu_finalize_phi(self._h, dptr(x), dptr(phi)))
+        return phi
+
+    def energy(self, phi: np.ndarray) -> np.ndarray:
+        phi = np.asfortranarray(phi, dtype=np.float64)
+        w = np.zeros(3)
+        check(_lib.lib().pot3d_gpu_energy(self._h, dptr(phi), dptr(w)))
+        return w
+
+    # ---- kernel-level entry points (device tensors) ---------------------
+    def ax_dev(self, x, y):
+        check(_lib.lib().pot3d_gpu_ax_dev(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())))
+
+    def prec_dev(self, x):
+        check(_lib.lib().pot3d_gpu_prec_dev(self._h, C.c_void_p(x.data_ptr())))
+
+    def time_kernels(self, reps: int = 20):
+        """Average ms per launch of the stencil and update kernels, and their
+        algorithmic DRAM bytes per launch."""
+        ms = np.zeros(2)
+        by = np.zeros(2)
+        check(_lib.lib().pot3d_gpu_time_kernels(self._h, reps, dptr(ms), dptr(by)))
+        return ms, by
+
+    def precond_diag(self):
+        d = np.zeros(self.N, np.float32)
+        di = np.zeros(self.N, np.float32)
+        check(_lib.lib().pot3d_gpu_precond_diag(self._h, fptr(d), fptr(di)))
+        return d, di
+
+
+def ernorm_lines(history, ncghist: int, epscg: float):
+    """The convergence lines ernorm writes to pot3d.out
+    (src/pot3d.F90:4435-4464): every ncghist iterations and the last one."""
+    out = []
+    n = len(history)
+    for it in range(n):
+        last = it == n - 1 and history[it] < epscg
+        if (ncghist > 0 and it % ncghist == 0) or (last and ncghist > 0):
+            out.append(f" Iteration: {it:8d}   Residual: {history[it]:23.15E}")
+    return out
+
+
+def potfld(mesh: Mesh, br0, option="ss", ifprec=1, precision="fp64", epscg=1e-9, ncgmax=10_000_000, x0=None):
+    """The reference's potfld on the GPU: returns phi (with ghosts), the
+    energies (W_r, W_t, W_p), iteration count, epsn and the history."""
+    with Pot3dSolver(mesh, br0, option=option, ifprec=ifprec, precision=precision) as s:
+        b = s.rhs()
+        x = np.zeros(s.N) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        r = b.copy()
+        ierr = s.cgsolve(x, r, ncgmax=ncgmax, epscg=epscg)
+        info = s.last_info
+        phi = s.finalize_phi(x)
+        w = s.energy(phi)
+        return dict(x=x, r=r, rhs=b, ierr=ierr, ncg=info.ncg, epsn=info.epsn, true_resid=info.true_resid,
+                    seconds=info.seconds, n_refine=info.n_refine, launches=info.kernel_launches, phi=phi, energy=w,
+                    history=s.history())
