@@ -23,6 +23,7 @@
 
 #include "pot3d_internal.cuh"
 #include "pot3d_solver.h"
+#include "tma.cuh"
 
 using namespace pot3d;
 
@@ -136,37 +137,60 @@ struct StencilArgs {
   double *partials;
 };
 
-template <int MODE>
-__device__ __forceinline__ double2 pnew2(const StencilArgs &a, long long idx, double beta) {
-  if (MODE == MODE_AX) {
-    return __ldg(reinterpret_cast<const double2 *>(a.x + idx));
-  } else if (MODE == MODE_PCG) {
-    const double2 po = __ldg(reinterpret_cast<const double2 *>(a.p_old + idx));
-    const double2 rv = __ldg(reinterpret_cast<const double2 *>(a.r + idx));
-    const float2 av = __ldg(reinterpret_cast<const float2 *>(a.ai + idx));
-    return make_double2(fma(beta, po.x, (double)av.x * rv.x), fma(beta, po.y, (double)av.y * rv.y));
-  } else {
-    const double2 po = __ldg(reinterpret_cast<const double2 *>(a.p_old + idx));
-    const float2 zv = __ldg(reinterpret_cast<const float2 *>(a.z32 + idx));
-    return make_double2(fma(beta, po.x, (double)zv.x), fma(beta, po.y, (double)zv.y));
-  }
-}
-template <int MODE>
-__device__ __forceinline__ double pnew1(const StencilArgs &a, long long idx, double beta) {
-  if (MODE == MODE_AX) {
-    return __ldg(a.x + idx);
-  } else if (MODE == MODE_PCG) {
-    return fma(beta, __ldg(a.p_old + idx), (double)__ldg(a.ai + idx) * __ldg(a.r + idx));
-  } else {
-    return fma(beta, __ldg(a.p_old + idx), (double)__ldg(a.z32 + idx));
-  }
-}
+// Shared-memory layout of the TMA-staged stencil.  Each pipeline stage holds
+// one k-plane of the tile plus a one-point halo: FP64 boxes of 68 x 10
+// points starting at (i = ib-2, j = j0-1) and FP32 boxes of 72 x 10 starting
+// at (i = ib-4, j = j0-1), so every TMA x-coordinate is 16-byte aligned.
+// Rows or columns outside the vector are zero-filled by the TMA unit; the
+// physical ghosts are applied when the stencil is evaluated.
+constexpr int S_STAGES = 4;
+constexpr int BOX_Y = TJ + 2;
+constexpr int BOX64_X = TI + 4;
+constexpr int BOX32_X = TI + 8;
+constexpr int TILE64_BYTES = BOX64_X * BOX_Y * 8;
+constexpr int TILE32_BYTES = BOX32_X * BOX_Y * 4;
+constexpr int TILE64_PITCH = (TILE64_BYTES + 127) / 128 * 128;
+constexpr int TILE32_PITCH = (TILE32_BYTES + 127) / 128 * 128;
+constexpr int PN_SLOTS = 4;
+constexpr uint32_t WAIT_LIMIT = 1u << 24;
 
 template <int MODE>
-__global__ void __launch_bounds__(NTHR, 2) k_stencil(Geo g, DevMesh m, StencilArgs a) {
-  __shared__ __align__(16) double tile[2][TJ + 2][SROW];
+struct StageCfg;
+template <>
+struct StageCfg<MODE_AX> {
+  static constexpr int n64 = 1, n32 = 0;
+};
+template <>
+struct StageCfg<MODE_PCG> {
+  static constexpr int n64 = 2, n32 = 1;
+};
+template <>
+struct StageCfg<MODE_PCGZ> {
+  static constexpr int n64 = 1, n32 = 1;
+};
+template <int MODE>
+struct StageLayout {
+  static constexpr int n64 = StageCfg<MODE>::n64, n32 = StageCfg<MODE>::n32;
+  static constexpr int bytes = n64 * TILE64_PITCH + n32 * TILE32_PITCH;
+  static constexpr uint32_t tx = n64 * TILE64_BYTES + n32 * TILE32_BYTES;
+  static constexpr int smem = S_STAGES * bytes + PN_SLOTS * TILE64_BYTES + 128;
+};
+
+// Tensor maps of the stage inputs: m64[0] = x | p_old, m64[1] = r, m32 = a_i | z.
+struct StencilMaps {
+  CUtensorMap m64[2];
+  CUtensorMap m32;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(NTHR, 2)
+    k_stencil(const __grid_constant__ StencilMaps maps, Geo g, DevMesh m, StencilArgs a) {
+  using L = StageLayout<MODE>;
+  extern __shared__ __align__(1024) unsigned char dyn[];
+  __shared__ __align__(8) uint64_t bar[S_STAGES];
   __shared__ double red[NTHR / 32];
   __shared__ double s1sh[TI];
+  __shared__ int abort_flag;
 
   double beta = 0.0;
   int par = 0;
@@ -176,12 +200,16 @@ __global__ void __launch_bounds__(NTHR, 2) k_stencil(Geo g, DevMesh m, StencilAr
     beta = vs->beta;
     par = vs->par;
   }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~uintptr_t(127));
+  double *pn_ring = reinterpret_cast<double *>(base + S_STAGES * L::bytes);  // [PN_SLOTS][BOX_Y][BOX64_X]
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5;
   const int ib = blockIdx.x * TI;
-  const int el = 2 * lane;          // local column of my first element
-  const int e0 = ib + el;           // interior radial offset (Fortran i = e0+2)
+  const int el = 2 * lane;
+  const int e0 = ib + el;
   const int j0 = blockIdx.y * TJ;
-  const int jj = j0 + w;            // interior theta offset (Fortran j = jj+2)
+  const int jj = j0 + w;
   const int k0 = blockIdx.z * g.tk;
   const int k1 = min(k0 + g.tk, g.npm2);
   const bool rowv = jj < g.ntm2;
@@ -189,25 +217,49 @@ __global__ void __launch_bounds__(NTHR, 2) k_stencil(Geo g, DevMesh m, StencilAr
   const bool v1 = rowv && e0 + 1 < g.nrm2;
   const bool south = rowv && jj == g.ntm2 - 1;
 
-  // South-pole ring sums for my two radial points (only the last row).
-  if (threadIdx.x < TI) s1sh[threadIdx.x] = 0.0;
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < S_STAGES; s++) mbar_init(&bar[s], 1);
+    mbar_init_fence();
+    tma_prefetch_desc(&maps.m64[0]);
+    if (L::n64 > 1) tma_prefetch_desc(&maps.m64[1]);
+    if (L::n32 > 0) tma_prefetch_desc(&maps.m32);
+  }
+  if (tid < TI) s1sh[tid] = 0.0;
   __syncthreads();
+
+  const int p_first = k0 - 1;         // planes p_first .. k1 feed the stencil
+  const int n_planes = k1 - k0 + 2;
+  auto issue = [&](int local) {       // thread 0: TMA loads of one plane
+    const int p = p_first + local;
+    const int kk = (p + g.npm2) % g.npm2;
+    const int s = local % S_STAGES;
+    unsigned char *st = base + s * L::bytes;
+    mbar_expect_tx(&bar[s], L::tx);
+    tma_load_3d(st, &maps.m64[0], ib - 2, j0 - 1, kk, &bar[s]);
+    if (L::n64 > 1) tma_load_3d(st + TILE64_PITCH, &maps.m64[1], ib - 2, j0 - 1, kk, &bar[s]);
+    if (L::n32 > 0) tma_load_3d(st + L::n64 * TILE64_PITCH, &maps.m32, ib - 4, j0 - 1, kk, &bar[s]);
+  };
+  int issued = 0;
+  if (tid == 0) {
+    for (; issued < S_STAGES && issued < n_planes; issued++) issue(issued);
+  }
+
+  // South-pole ring sums for the tile's radial points (last theta row only).
   if (MODE == MODE_AX) {
-    if (threadIdx.x < TI && ib + threadIdx.x < g.nrm2) s1sh[threadIdx.x] = a.s1_direct[ib + threadIdx.x];
+    if (tid < TI && ib + tid < g.nrm2) s1sh[tid] = a.s1_direct[ib + tid];
   } else if (j0 + TJ >= g.ntm2) {
     // S1(p_new) = beta*S1(p_old) + S1(z): the ring sums are linear in p.
-    if (threadIdx.x < TI && ib + threadIdx.x < g.nrm2) {
-      const int e = ib + threadIdx.x;
+    if (tid < TI && ib + tid < g.nrm2) {
+      const int e = ib + tid;
       double sz = 0.0;
       for (int c = 0; c < g.nkc; c++) sz += a.s1z_part[(long long)c * g.NRP + e];
       const double s = fma(beta, a.s1p[par * g.NRP + e], sz);
-      s1sh[threadIdx.x] = s;
+      s1sh[tid] = s;
       if (blockIdx.z == 0) a.s1p[(par ^ 1) * g.NRP + e] = s;
     }
   }
-  __syncthreads();
 
-  // Per-thread coefficient factors.
   const int jf = jj + 2;
   RowCoef rc;
   PtCoef pc0, pc1;
@@ -216,83 +268,103 @@ __global__ void __launch_bounds__(NTHR, 2) k_stencil(Geo g, DevMesh m, StencilAr
     pc0 = pt_coef(m, min(e0, g.nrm2 - 1) + 2, jf);
     pc1 = pt_coef(m, min(e0 + 1, g.nrm2 - 1) + 2, jf);
   }
+  __syncthreads();
   const double s1a = south ? s1sh[el] : 0.0, s1b = south ? s1sh[el + 1] : 0.0;
-
-  // Prologue: planes k0-1 (periodic wrap) and k0.
-  const int km0 = (k0 == 0) ? g.npm2 - 1 : k0 - 1;
-  double2 xm = make_double2(0.0, 0.0), xc = xm, xn = xm;
-  if (v0) {
-    xm = pnew2<MODE>(a, g.idx(e0, jj, km0), beta);
-    xc = pnew2<MODE>(a, g.idx(e0, jj, k0), beta);
-  }
-  double dot = 0.0;
   const double pm = m.pm_r1;
+  double dot = 0.0;
 
-  for (int kk = k0; kk < k1; kk++) {
-    const int buf = kk & 1;
-    const int kn = (kk + 1 == g.npm2) ? 0 : kk + 1;
-    if (v0) xn = pnew2<MODE>(a, g.idx(e0, jj, kn), beta);
-    // Own values of plane kk into shared memory (pad element zeroed).
-    double2 own = xc;
-    if (!v1) own.y = 0.0;
-    if (!v0) own.x = 0.0;
-    *reinterpret_cast<double2 *>(&tile[buf][w + 1][2 + el]) = own;
-    // Theta halo rows (interior neighbours only; ghosts are applied below).
-    if (w == 0 || w == TJ - 1) {
-      const int jh = (w == 0) ? j0 - 1 : j0 + TJ;
+  // p_new at (row, col) of the stage tile; col counts FP64 columns.
+  auto pnew_at = [&](const unsigned char *st, int row, int col) -> double {
+    const double *t0 = reinterpret_cast<const double *>(st);
+    if (MODE == MODE_AX) {
+      return t0[row * BOX64_X + col];
+    } else if (MODE == MODE_PCG) {
+      const double *t1 = reinterpret_cast<const double *>(st + TILE64_PITCH);
+      const float *t2 = reinterpret_cast<const float *>(st + 2 * TILE64_PITCH);
+      return fma(beta, t0[row * BOX64_X + col], (double)t2[row * BOX32_X + col + 2] * t1[row * BOX64_X + col]);
+    } else {
+      const float *t2 = reinterpret_cast<const float *>(st + TILE64_PITCH);
+      return fma(beta, t0[row * BOX64_X + col], (double)t2[row * BOX32_X + col + 2]);
+    }
+  };
+
+  int local = 0;
+  for (; local < n_planes; local++) {
+    const int s = local % S_STAGES;
+    const uint32_t parity = (local / S_STAGES) & 1;
+    if (!mbar_wait(&bar[s], parity, WAIT_LIMIT)) abort_flag = 1;
+    const unsigned char *st = base + s * L::bytes;
+    double *slot = pn_ring + (local % PN_SLOTS) * (BOX_Y * BOX64_X);
+    // own pair
+    {
+      const int col = 2 + el;
+      slot[(w + 1) * BOX64_X + col] = pnew_at(st, w + 1, col);
+      slot[(w + 1) * BOX64_X + col + 1] = pnew_at(st, w + 1, col + 1);
+    }
+    if (w == 0 || w == TJ - 1) {  // theta halo rows
       const int row = (w == 0) ? 0 : TJ + 1;
-      double2 hv = make_double2(0.0, 0.0);
-      if (jh >= 0 && jh < g.ntm2 && e0 < g.nrm2) hv = pnew2<MODE>(a, g.idx(e0, jh, kk), beta);
-      *reinterpret_cast<double2 *>(&tile[buf][row][2 + el]) = hv;
+      const int col = 2 + el;
+      slot[row * BOX64_X + col] = pnew_at(st, row, col);
+      slot[row * BOX64_X + col + 1] = pnew_at(st, row, col + 1);
     }
-    // Radial halo columns.
-    if (lane == 0) {
-      double hv = 0.0;
-      if (rowv && ib > 0) hv = pnew1<MODE>(a, g.idx(ib - 1, jj, kk), beta);
-      tile[buf][w + 1][1] = hv;
-    } else if (lane == 31) {
-      double hv = 0.0;
-      if (rowv && ib + TI < g.nrm2) hv = pnew1<MODE>(a, g.idx(ib + TI, jj, kk), beta);
-      tile[buf][w + 1][TI + 2] = hv;
-    }
+    if (lane == 0) slot[(w + 1) * BOX64_X + 1] = pnew_at(st, w + 1, 1);
+    if (lane == 31) slot[(w + 1) * BOX64_X + TI + 2] = pnew_at(st, w + 1, TI + 2);
     __syncthreads();
-    if (v0) {
+    if (abort_flag) break;
+    if (tid == 0 && issued < n_planes) {  // refill the stage just consumed
+      issue(issued);
+      issued++;
+    }
+    if (local >= 2 && v0) {
+      const int kk = p_first + local - 1;  // plane whose stencil is now complete
+      const double *sc = pn_ring + ((local - 1) % PN_SLOTS) * (BOX_Y * BOX64_X);
+      const double *sm = pn_ring + ((local - 2) % PN_SLOTS) * (BOX_Y * BOX64_X);
+      const double *sp = slot;
       const int kf = kk + 2;
       const double dpim = m.dp_i[kf - 1], dpip = m.dp_i[kf], dphk = m.dph[kf];
-      const double *trow = tile[buf][w + 1];
-      // element 0
-      {
-        const Coef7 c = coef7(pc0, rc, dpim, dpip, dphk);
-        const double xim = (e0 == 0) ? xc.x : trow[1 + el];
-        const double xip = (e0 == g.nrm2 - 1) ? pm * xc.x : xc.y;
-        const double xjm = (jj == 0) ? 0.0 : tile[buf][w][2 + el];
-        const double xjp = south ? 2.0 * s1a - xc.x : tile[buf][w + 2][2 + el];
-        const double y = apply7(c, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
-        double y1 = 0.0;
-        if (v1) {
-          const Coef7 c1 = coef7(pc1, rc, dpim, dpip, dphk);
-          const double xim1 = xc.x;
-          const double xip1 = (e0 + 1 == g.nrm2 - 1) ? pm * xc.y : trow[2 + el + 2];
-          const double xjm1 = (jj == 0) ? 0.0 : tile[buf][w][2 + el + 1];
-          const double xjp1 = south ? 2.0 * s1b - xc.y : tile[buf][w + 2][2 + el + 1];
-          y1 = apply7(c1, xm.y, xjm1, xim1, xc.y, xip1, xjp1, xn.y);
-        }
-        const long long id = g.idx(e0, jj, kk);
-        const double2 yv = make_double2(y, y1);
-        if (MODE == MODE_AX) {
-          *reinterpret_cast<double2 *>(a.y + id) = yv;
-        } else {
-          *reinterpret_cast<double2 *>(a.q + id) = yv;
-          *reinterpret_cast<double2 *>(a.p_new + id) = own;
-          dot = fma(own.x, y, dot);
-          dot = fma(own.y, y1, dot);
-        }
+      const int col = 2 + el;
+      const double *rowc = sc + (w + 1) * BOX64_X;
+      const double2 xc = *reinterpret_cast<const double2 *>(rowc + col);
+      const double2 xm = *reinterpret_cast<const double2 *>(sm + (w + 1) * BOX64_X + col);
+      const double2 xn = *reinterpret_cast<const double2 *>(sp + (w + 1) * BOX64_X + col);
+      const double2 xjm2 = *reinterpret_cast<const double2 *>(sc + w * BOX64_X + col);
+      const double2 xjp2 = *reinterpret_cast<const double2 *>(sc + (w + 2) * BOX64_X + col);
+      const Coef7 c = coef7(pc0, rc, dpim, dpip, dphk);
+      const double xim = (e0 == 0) ? xc.x : rowc[col - 1];
+      const double xip = (e0 == g.nrm2 - 1) ? pm * xc.x : xc.y;
+      const double xjm = (jj == 0) ? 0.0 : xjm2.x;
+      const double xjp = south ? 2.0 * s1a - xc.x : xjp2.x;
+      const double y = apply7(c, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
+      double y1 = 0.0;
+      if (v1) {
+        const Coef7 c1 = coef7(pc1, rc, dpim, dpip, dphk);
+        const double xip1 = (e0 + 1 == g.nrm2 - 1) ? pm * xc.y : rowc[col + 2];
+        const double xjm1 = (jj == 0) ? 0.0 : xjm2.y;
+        const double xjp1 = south ? 2.0 * s1b - xc.y : xjp2.y;
+        y1 = apply7(c1, xm.y, xjm1, xc.x, xc.y, xip1, xjp1, xn.y);
+      }
+      const long long id = g.idx(e0, jj, kk);
+      const double2 yv = make_double2(y, y1);
+      if (MODE == MODE_AX) {
+        *reinterpret_cast<double2 *>(a.y + id) = yv;
+      } else {
+        const double2 own = make_double2(xc.x, v1 ? xc.y : 0.0);
+        *reinterpret_cast<double2 *>(a.q + id) = yv;
+        *reinterpret_cast<double2 *>(a.p_new + id) = own;
+        dot = fma(own.x, y, dot);
+        dot = fma(own.y, y1, dot);
       }
     }
-    xm = xc;
-    xc = xn;
   }
 
+  if (abort_flag) {
+    // Drain the loads still in flight (bounded), report, and leave.
+    if (tid == 0) {
+      for (int l = local; l < issued; l++) mbar_wait(&bar[l % S_STAGES], (l / S_STAGES) & 1, WAIT_LIMIT);
+      if (MODE != MODE_AX) atomicExch(&a.st->status, ST_TIMEOUT);
+    }
+    return;
+  }
   if (MODE != MODE_AX) {
     double bs = block_sum<NTHR>(dot, red);
     double total;
@@ -677,6 +749,61 @@ __global__ void k_scale_ai(long long n, const float *__restrict__ ai, double *__
 // ============================================================================
 namespace pot3d {
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 3-D tensor map of a padded vector (i, j, k) = (NRP, ntm2, npm2) with the
+// stencil's box: 68 x 10 x 1 FP64 or 72 x 10 x 1 FP32.
+int Solver::tensor_map(const void *ptr, bool fp64, CUtensorMap *out) {
+  auto key = std::make_pair(ptr, fp64 ? 1 : 0);
+  auto it = tmaps.find(key);
+  if (it != tmaps.end()) {
+    *out = it->second;
+    return POT3D_OK;
+  }
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) {
+    pot3d_set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return POT3D_ERR_CUDA;
+  }
+  const cuuint64_t es = fp64 ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)g.NRP, (cuuint64_t)g.ntm2, (cuuint64_t)g.npm2};
+  cuuint64_t strides[2] = {(cuuint64_t)g.NRP * es, (cuuint64_t)g.NRP * g.ntm2 * es};
+  cuuint32_t box[3] = {(cuuint32_t)(fp64 ? BOX64_X : BOX32_X), (cuuint32_t)BOX_Y, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMap mp;
+  CUresult r = fn(&mp, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                  const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    pot3d_set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return POT3D_ERR_CUDA;
+  }
+  tmaps[key] = mp;
+  *out = mp;
+  return POT3D_OK;
+}
+
+template <int MODE>
+static int set_stencil_smem() {
+  return pot3d_cuda_status(cudaFuncSetAttribute(k_stencil<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                StageLayout<MODE>::smem),
+                           "cudaFuncSetAttribute(k_stencil)");
+}
+
 int grid1d(long long n) {
   long long b = (n + NTHR - 1) / NTHR;
   if (b > 148LL * 16) b = 148LL * 16;
@@ -757,6 +884,11 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   g.nkc = (g.npm2 + g.tk - 1) / g.tk;
 
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  {
+    int e;
+    if ((e = set_stencil_smem<MODE_AX>()) || (e = set_stencil_smem<MODE_PCG>()) || (e = set_stencil_smem<MODE_PCGZ>()))
+      return e;
+  }
   CK(cudaEventCreate(&ev0));
   CK(cudaEventCreate(&ev1));
   int st = POT3D_OK;
@@ -844,8 +976,13 @@ int Solver::ax_padded(const double *x, double *y) {
   a.x = x;
   a.y = y;
   a.s1_direct = d_s1;
+  StencilMaps mp;
+  int st;
+  if ((st = tensor_map(x, true, &mp.m64[0]))) return st;
+  mp.m64[1] = mp.m64[0];
+  mp.m32 = mp.m64[0];
   dim3 grid(g.nit, g.njt, g.nkc);
-  k_stencil<MODE_AX><<<grid, NTHR, 0, stream>>>(g, m, a);
+  k_stencil<MODE_AX><<<grid, NTHR, StageLayout<MODE_AX>::smem, stream>>>(mp, g, m, a);
   return pot3d_cuda_status(cudaGetLastError(), "k_stencil<AX>");
 }
 
@@ -900,9 +1037,14 @@ int Solver::launch_iteration() {
   ua.s1z_part = d_s1z;
   ua.st = d_state;
   ua.partials = d_partials;
+  StencilMaps mp;
+  int stm;
+  if ((stm = tensor_map(p_cur, true, &mp.m64[0]))) return stm;
   if (ifprec == 2) {
     sa.z32 = dilu_z32(this);
-    k_stencil<MODE_PCGZ><<<grid, NTHR, 0, stream>>>(g, m, sa);
+    mp.m64[1] = mp.m64[0];
+    if ((stm = tensor_map(sa.z32, false, &mp.m32))) return stm;
+    k_stencil<MODE_PCGZ><<<grid, NTHR, StageLayout<MODE_PCGZ>::smem, stream>>>(mp, g, m, sa);
     ua.r32 = dilu_r32(this);
     k_update_r32<<<grid1d(g.Np / 2), NTHR, 0, stream>>>(g, ua);
     int st = dilu_sweeps(this, true);
@@ -910,7 +1052,9 @@ int Solver::launch_iteration() {
     ua.z32 = dilu_z32(this);
     k_update<UPD_ZDOT, true><<<grid, NTHR, 0, stream>>>(g, m, ua);
   } else {
-    k_stencil<MODE_PCG><<<grid, NTHR, 0, stream>>>(g, m, sa);
+    if ((stm = tensor_map(d_r, true, &mp.m64[1]))) return stm;
+    if ((stm = tensor_map(d_ai, false, &mp.m32))) return stm;
+    k_stencil<MODE_PCG><<<grid, NTHR, StageLayout<MODE_PCG>::smem, stream>>>(mp, g, m, sa);
     k_update<UPD_ITER, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
   }
   std::swap(p_cur, p_nxt);
@@ -1052,6 +1196,10 @@ int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr,
     pot3d_set_error("PCG breakdown (non-finite or zero p.Ap)");
     return POT3D_ERR_BREAKDOWN;
   }
+  if (h_state->status == ST_TIMEOUT) {
+    pot3d_set_error("a bounded wait for a TMA tile ran out in the stencil kernel");
+    return POT3D_ERR_TIMEOUT;
+  }
   *ierr = (h_state->status == ST_CONVERGED) ? 0 : 1;
   if (info) {
     info->ncg = last_ncg;
@@ -1104,8 +1252,13 @@ int Solver::time_kernels(int reps, double ms[2], double bytes[2]) {
     sa.st = d_state;
     sa.partials = d_partials;
     ua.p = p_nxt;
+    StencilMaps mp;
+    int stm;
+    if ((stm = tensor_map(p_cur, true, &mp.m64[0])) || (stm = tensor_map(d_r, true, &mp.m64[1])) ||
+        (stm = tensor_map(d_ai, false, &mp.m32)))
+      return stm;
     CK(cudaEventRecord(e[0], stream));
-    k_stencil<MODE_PCG><<<grid, NTHR, 0, stream>>>(g, m, sa);
+    k_stencil<MODE_PCG><<<grid, NTHR, StageLayout<MODE_PCG>::smem, stream>>>(mp, g, m, sa);
     CK(cudaEventRecord(e[1], stream));
     k_update<UPD_ITER, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
     CK(cudaEventRecord(e[2], stream));

@@ -58,7 +58,7 @@ struct SolveState {
   double *hist;
 };
 
-enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXIT = 2, ST_BREAKDOWN = 3 };
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXIT = 2, ST_BREAKDOWN = 3, ST_TIMEOUT = 4 };
 
 // ---- deterministic block reduction --------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {

@@ -1,8 +1,11 @@
 // Host-side solver object behind the pot3d_gpu_* C-ABI.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <map>
+#include <utility>
 #include <vector>
 
 #include "pot3d_internal.cuh"
@@ -42,6 +45,10 @@ struct Solver {
   long long launches = 0;  // kernel launches of the last solve
   int last_ncg = 0, last_refine = 0;
   double last_epsn = 0.0, last_seconds = 0.0;
+
+  // TMA descriptors of padded vectors, keyed by (address, is_fp64).
+  std::map<std::pair<const void *, int>, CUtensorMap> tmaps;
+  int tensor_map(const void *ptr, bool fp64, CUtensorMap *out);
 
   DiluState *dilu = nullptr;
   MixedState *mixed = nullptr;
