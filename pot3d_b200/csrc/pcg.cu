@@ -106,6 +106,41 @@ __device__ __forceinline__ double apply7(const Coef7 &a, double xkm, double xjm,
   return y;
 }
 
+// The stencil kernels use the coefficients in factored form: with
+//   g1 = drh*dth*sth_i, g2 = drh*st(j-1)*dt_i(j-1), g6 = drh*st(j)*dt_i(j),
+//   g3 = sth*dth*r2(i-1)*dr_i(i-1), g5 = sth*dth*r2(i)*dr_i(i)
+// the seven coefficients of load_matrix_pot3d_solve are
+//   a1 = -g1*dp_i(k-1), a7 = -g1*dp_i(k), a2 = -g2*dph(k), a6 = -g6*dph(k),
+//   a3 = -g3*dph(k), a5 = -g5*dph(k), a4 = -(a1+a2+a3+a5+a6+a7),
+// so y = a4*x - g1*(dp_i(k-1)*x(k-1) + dp_i(k)*x(k+1))
+//          - dph(k)*(g2*x(j-1) + g3*x(i-1) + g5*x(i+1) + g6*x(j+1)).
+// This evaluates the same operator with short dependency chains; values
+// differ from the stored-coefficient form by rounding only.
+struct PtFac {
+  double g1, g2, g3, g5, g6, gs;  // gs = g2+g3+g5+g6
+};
+__device__ __forceinline__ PtFac pt_fac(const DevMesh &m, int i, int j) {
+  PtFac f;
+  const double drh = m.drh[i];
+  const double sd = m.sth[j] * m.dth[j];
+  f.g1 = drh * m.dth[j] * m.sth_i[j];
+  f.g2 = drh * m.st[j - 1] * m.dt_i[j - 1];
+  f.g6 = drh * m.st[j] * m.dt_i[j];
+  f.g3 = sd * m.r2[i - 1] * m.dr_i[i - 1];
+  f.g5 = sd * m.r2[i] * m.dr_i[i];
+  f.gs = (f.g2 + f.g6) + (f.g3 + f.g5);
+  return f;
+}
+__device__ __forceinline__ double apply_fac(const PtFac &f, double dpim, double dpip, double dphk, double xkm,
+                                            double xjm, double xim, double xc, double xip, double xjp, double xkp) {
+  const double a4 = fma(f.g1, dpim + dpip, f.gs * dphk);
+  const double tk = fma(dpim, xkm, dpip * xkp);
+  const double tr = fma(f.g3, xim, f.g5 * xip);
+  const double tt = fma(f.g2, xjm, f.g6 * xjp);
+  const double off = fma(f.g1, tk, dphk * (tr + tt));
+  return fma(a4, xc, -off);
+}
+
 // ============================================================================
 // Stencil kernel.  MODE_AX: y = A x (ax, src/pot3d.F90:5102-5150) with the
 // south-pole ring sums S1 supplied.  MODE_PCG: p_new = beta*p + a_i*r on the
@@ -152,6 +187,7 @@ constexpr int TILE32_BYTES = BOX32_X * BOX_Y * 4;
 constexpr int TILE64_PITCH = (TILE64_BYTES + 127) / 128 * 128;
 constexpr int TILE32_PITCH = (TILE32_BYTES + 127) / 128 * 128;
 constexpr int PN_SLOTS = 4;
+constexpr int MAX_TK = 512;  // k-planes per block at most (per-k factors in shared memory)
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
 
 template <int MODE>
@@ -173,7 +209,8 @@ struct StageLayout {
   static constexpr int n64 = StageCfg<MODE>::n64, n32 = StageCfg<MODE>::n32;
   static constexpr int bytes = n64 * TILE64_PITCH + n32 * TILE32_PITCH;
   static constexpr uint32_t tx = n64 * TILE64_BYTES + n32 * TILE32_BYTES;
-  static constexpr int smem = S_STAGES * bytes + PN_SLOTS * TILE64_BYTES + 128;
+  static constexpr int kfac_off = S_STAGES * bytes + PN_SLOTS * TILE64_BYTES + 128;
+  static constexpr int smem = kfac_off + 3 * 8 * MAX_TK;
 };
 
 // Tensor maps of the stage inputs: m64[0] = x | p_old, m64[1] = r, m32 = a_i | z.
@@ -200,6 +237,7 @@ __global__ void __launch_bounds__(NTHR, 2)
     beta = vs->beta;
     par = vs->par;
   }
+  double *kfac = reinterpret_cast<double *>(dyn + L::kfac_off);  // [tk][3]
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~uintptr_t(127));
   double *pn_ring = reinterpret_cast<double *>(base + S_STAGES * L::bytes);  // [PN_SLOTS][BOX_Y][BOX64_X]
 
@@ -253,7 +291,7 @@ __global__ void __launch_bounds__(NTHR, 2)
     if (tid < TI && ib + tid < g.nrm2) {
       const int e = ib + tid;
       double sz = 0.0;
-      for (int c = 0; c < g.nkc; c++) sz += a.s1z_part[(long long)c * g.NRP + e];
+      for (int c = 0; c < g.nkc_u; c++) sz += a.s1z_part[(long long)c * g.NRP + e];
       const double s = fma(beta, a.s1p[par * g.NRP + e], sz);
       s1sh[tid] = s;
       if (blockIdx.z == 0) a.s1p[(par ^ 1) * g.NRP + e] = s;
@@ -261,12 +299,17 @@ __global__ void __launch_bounds__(NTHR, 2)
   }
 
   const int jf = jj + 2;
-  RowCoef rc;
-  PtCoef pc0, pc1;
+  PtFac f0, f1;
   if (rowv) {
-    rc = row_coef(m, jf);
-    pc0 = pt_coef(m, min(e0, g.nrm2 - 1) + 2, jf);
-    pc1 = pt_coef(m, min(e0 + 1, g.nrm2 - 1) + 2, jf);
+    f0 = pt_fac(m, min(e0, g.nrm2 - 1) + 2, jf);
+    f1 = pt_fac(m, min(e0 + 1, g.nrm2 - 1) + 2, jf);
+  }
+  // dp_i(k-1), dp_i(k), dph(k) of the block's planes, staged once.
+  for (int q = tid; q < k1 - k0; q += NTHR) {
+    const int kf = k0 + q + 2;
+    kfac[3 * q + 0] = m.dp_i[kf - 1];
+    kfac[3 * q + 1] = m.dp_i[kf];
+    kfac[3 * q + 2] = m.dph[kf];
   }
   __syncthreads();
   const double s1a = south ? s1sh[el] : 0.0, s1b = south ? s1sh[el + 1] : 0.0;
@@ -301,14 +344,18 @@ __global__ void __launch_bounds__(NTHR, 2)
       slot[(w + 1) * BOX64_X + col] = pnew_at(st, w + 1, col);
       slot[(w + 1) * BOX64_X + col + 1] = pnew_at(st, w + 1, col + 1);
     }
-    if (w == 0 || w == TJ - 1) {  // theta halo rows
-      const int row = (w == 0) ? 0 : TJ + 1;
-      const int col = 2 + el;
-      slot[row * BOX64_X + col] = pnew_at(st, row, col);
-      slot[row * BOX64_X + col + 1] = pnew_at(st, row, col + 1);
+    {  // halo: theta rows 0 and TJ+1 (128 points) and radial columns (16)
+      if (tid < 2 * TI) {
+        const int row = (tid < TI) ? 0 : TJ + 1;
+        const int col = 2 + (tid & (TI - 1));
+        slot[row * BOX64_X + col] = pnew_at(st, row, col);
+      } else if (tid < 2 * TI + 2 * TJ) {
+        const int q = tid - 2 * TI;
+        const int row = 1 + (q >> 1);
+        const int col = (q & 1) ? TI + 2 : 1;
+        slot[row * BOX64_X + col] = pnew_at(st, row, col);
+      }
     }
-    if (lane == 0) slot[(w + 1) * BOX64_X + 1] = pnew_at(st, w + 1, 1);
-    if (lane == 31) slot[(w + 1) * BOX64_X + TI + 2] = pnew_at(st, w + 1, TI + 2);
     __syncthreads();
     if (abort_flag) break;
     if (tid == 0 && issued < n_planes) {  // refill the stage just consumed
@@ -320,8 +367,8 @@ __global__ void __launch_bounds__(NTHR, 2)
       const double *sc = pn_ring + ((local - 1) % PN_SLOTS) * (BOX_Y * BOX64_X);
       const double *sm = pn_ring + ((local - 2) % PN_SLOTS) * (BOX_Y * BOX64_X);
       const double *sp = slot;
-      const int kf = kk + 2;
-      const double dpim = m.dp_i[kf - 1], dpip = m.dp_i[kf], dphk = m.dph[kf];
+      const int kq = kk - k0;
+      const double dpim = kfac[3 * kq], dpip = kfac[3 * kq + 1], dphk = kfac[3 * kq + 2];
       const int col = 2 + el;
       const double *rowc = sc + (w + 1) * BOX64_X;
       const double2 xc = *reinterpret_cast<const double2 *>(rowc + col);
@@ -329,19 +376,17 @@ __global__ void __launch_bounds__(NTHR, 2)
       const double2 xn = *reinterpret_cast<const double2 *>(sp + (w + 1) * BOX64_X + col);
       const double2 xjm2 = *reinterpret_cast<const double2 *>(sc + w * BOX64_X + col);
       const double2 xjp2 = *reinterpret_cast<const double2 *>(sc + (w + 2) * BOX64_X + col);
-      const Coef7 c = coef7(pc0, rc, dpim, dpip, dphk);
       const double xim = (e0 == 0) ? xc.x : rowc[col - 1];
       const double xip = (e0 == g.nrm2 - 1) ? pm * xc.x : xc.y;
       const double xjm = (jj == 0) ? 0.0 : xjm2.x;
       const double xjp = south ? 2.0 * s1a - xc.x : xjp2.x;
-      const double y = apply7(c, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
+      const double y = apply_fac(f0, dpim, dpip, dphk, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
       double y1 = 0.0;
       if (v1) {
-        const Coef7 c1 = coef7(pc1, rc, dpim, dpip, dphk);
         const double xip1 = (e0 + 1 == g.nrm2 - 1) ? pm * xc.y : rowc[col + 2];
         const double xjm1 = (jj == 0) ? 0.0 : xjm2.y;
         const double xjp1 = south ? 2.0 * s1b - xc.y : xjp2.y;
-        y1 = apply7(c1, xm.y, xjm1, xc.x, xc.y, xip1, xjp1, xn.y);
+        y1 = apply_fac(f1, dpim, dpip, dphk, xm.y, xjm1, xc.x, xc.y, xip1, xjp1, xn.y);
       }
       const long long id = g.idx(e0, jj, kk);
       const double2 yv = make_double2(y, y1);
@@ -416,13 +461,14 @@ __global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a)
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int e0 = blockIdx.x * TI + 2 * lane;
   const int jj = blockIdx.y * TJ + w;
-  const int k0 = blockIdx.z * g.tk;
-  const int k1 = min(k0 + g.tk, g.npm2);
+  const int k0 = blockIdx.z * g.tk_u;
+  const int k1 = min(k0 + g.tk_u, g.npm2);
   const bool v0 = jj < g.ntm2 && e0 < g.nrm2;
   const bool v1 = v0 && e0 + 1 < g.nrm2;
   const bool south = v0 && jj == g.ntm2 - 1;
   double rz = 0.0, s1a = 0.0, s1b = 0.0;
   if (v0) {
+#pragma unroll 4
     for (int kk = k0; kk < k1; kk++) {
       const long long id = g.idx(e0, jj, kk);
       double2 rv = *reinterpret_cast<const double2 *>(a.r + id);
@@ -876,18 +922,41 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   g.Np = (long long)g.NRP * g.ntm2 * g.npm2;
   g.nit = (g.nrm2 + TI - 1) / TI;
   g.njt = (g.ntm2 + TJ - 1) / TJ;
-  // k-chunking: about six resident tile blocks per SM, one wave.
-  const long long cols = (long long)g.nit * g.njt;
-  const long long want = 148LL * 6;
-  int nkc = (int)std::max(1LL, std::min<long long>(g.npm2, (want + cols - 1) / cols));
-  g.tk = (g.npm2 + nkc - 1) / nkc;
-  g.nkc = (g.npm2 + g.tk - 1) / g.tk;
 
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   {
     int e;
     if ((e = set_stencil_smem<MODE_AX>()) || (e = set_stencil_smem<MODE_PCG>()) || (e = set_stencil_smem<MODE_PCGZ>()))
       return e;
+  }
+  // k-chunking by a wave model: the grid is (i tiles, j tiles, k chunks);
+  // pick the chunk count that minimises whole waves x planes per block,
+  // counting each block's pipeline start-up as extra planes.
+  {
+    int dev = 0, nsm = 148, occ_s = 2, occ_u = 8;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_stencil<MODE_PCG>, NTHR, StageLayout<MODE_PCG>::smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k_update<UPD_ITER, false>, NTHR, 0));
+    const long long cols = (long long)g.nit * g.njt;
+    auto pick = [&](int slots_per_sm, double startup, int max_tk, int *tk, int *nkc) {
+      const double slots = (double)std::max(1, slots_per_sm) * nsm;
+      double best = 1e300;
+      for (int c = 1; c <= g.npm2; c++) {
+        const int t = (g.npm2 + c - 1) / c;
+        if (t > max_tk) continue;
+        const int cc = (g.npm2 + t - 1) / t;
+        const double waves = std::ceil((double)(cols * cc) / slots);
+        const double cost = waves * (t + startup);
+        if (cost < best - 1e-9) {
+          best = cost;
+          *tk = t;
+          *nkc = cc;
+        }
+      }
+    };
+    pick(occ_s, 6.0, MAX_TK, &g.tk, &g.nkc);
+    pick(occ_u, 2.0, 1 << 30, &g.tk_u, &g.nkc_u);
   }
   CK(cudaEventCreate(&ev0));
   CK(cudaEventCreate(&ev1));
@@ -932,9 +1001,9 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
 
   if ((st = alloc((void **)&d_state, sizeof(SolveState)))) return st;
   CK(cudaMallocHost(&h_state, sizeof(SolveState)));
-  nblk_tiled = (size_t)g.nit * g.njt * g.nkc;
+  nblk_tiled = (size_t)g.nit * g.njt * std::max(g.nkc, g.nkc_u);
   if ((st = alloc((void **)&d_partials, sizeof(double) * std::max<size_t>(nblk_tiled, 148 * 16 * 3)))) return st;
-  if ((st = alloc((void **)&d_s1z, sizeof(double) * (size_t)g.nkc * g.NRP))) return st;
+  if ((st = alloc((void **)&d_s1z, sizeof(double) * (size_t)g.nkc_u * g.NRP))) return st;
   if ((st = alloc((void **)&d_s1p, sizeof(double) * 2 * (size_t)g.NRP))) return st;
   if ((st = alloc((void **)&d_s1, sizeof(double) * (size_t)g.NRP))) return st;
   if ((st = alloc((void **)&d_scalar, sizeof(double) * 8))) return st;
@@ -982,6 +1051,7 @@ int Solver::ax_padded(const double *x, double *y) {
   mp.m64[1] = mp.m64[0];
   mp.m32 = mp.m64[0];
   dim3 grid(g.nit, g.njt, g.nkc);
+  dim3 gridu(g.nit, g.njt, g.nkc_u);
   k_stencil<MODE_AX><<<grid, NTHR, StageLayout<MODE_AX>::smem, stream>>>(mp, g, m, a);
   return pot3d_cuda_status(cudaGetLastError(), "k_stencil<AX>");
 }
@@ -1018,6 +1088,7 @@ int Solver::unpack(const double *pad_dev, double *ref_dev) {
 // One PCG iteration (src/pot3d.F90:4336-4365).
 int Solver::launch_iteration() {
   dim3 grid(g.nit, g.njt, g.nkc);
+  dim3 gridu(g.nit, g.njt, g.nkc_u);
   StencilArgs sa{};
   sa.p_old = p_cur;
   sa.p_new = p_nxt;  // ping-pong: neighbouring tiles still read p_old halos
@@ -1050,12 +1121,12 @@ int Solver::launch_iteration() {
     int st = dilu_sweeps(this, true);
     if (st) return st;
     ua.z32 = dilu_z32(this);
-    k_update<UPD_ZDOT, true><<<grid, NTHR, 0, stream>>>(g, m, ua);
+    k_update<UPD_ZDOT, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   } else {
     if ((stm = tensor_map(d_r, true, &mp.m64[1]))) return stm;
     if ((stm = tensor_map(d_ai, false, &mp.m32))) return stm;
     k_stencil<MODE_PCG><<<grid, NTHR, StageLayout<MODE_PCG>::smem, stream>>>(mp, g, m, sa);
-    k_update<UPD_ITER, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
+    k_update<UPD_ITER, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   }
   std::swap(p_cur, p_nxt);
   return pot3d_cuda_status(cudaGetLastError(), "launch_iteration");
@@ -1064,6 +1135,7 @@ int Solver::launch_iteration() {
 // FP64 PCG (cgsolve, src/pot3d.F90:4231-4369) on d_x (guess) and d_b (RHS).
 int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info) {
   dim3 grid(g.nit, g.njt, g.nkc);
+  dim3 gridu(g.nit, g.njt, g.nkc_u);
   int st;
   SolveState s0{};
   s0.epscg = epscg;
@@ -1092,9 +1164,9 @@ int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr,
     k_cast_r32<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_r, dilu_r32(this));
     if ((st = dilu_sweeps(this, false))) return st;
     ua.z32 = dilu_z32(this);
-    k_update<UPD_BDOTB, true><<<grid, NTHR, 0, stream>>>(g, m, ua);
+    k_update<UPD_BDOTB, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   } else {
-    k_update<UPD_BDOTB, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
+    k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   }
   launches += (ifprec == 2) ? 2 + sweep_launches() : 1;
   CK(cudaGetLastError());
@@ -1120,9 +1192,9 @@ int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr,
     k_cast_r32<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_r, dilu_r32(this));
     if ((st = dilu_sweeps(this, false))) return st;
     ua.z32 = dilu_z32(this);
-    k_update<UPD_INIT, true><<<grid, NTHR, 0, stream>>>(g, m, ua);
+    k_update<UPD_INIT, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   } else {
-    k_update<UPD_INIT, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
+    k_update<UPD_INIT, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   }
   launches += (ifprec == 2) ? 2 + sweep_launches() : 1;
   CK(cudaGetLastError());
@@ -1215,6 +1287,7 @@ int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr,
 // Stencil and update kernels of the FP64 diagonal PCG timed one by one.
 int Solver::time_kernels(int reps, double ms[2], double bytes[2]) {
   dim3 grid(g.nit, g.njt, g.nkc);
+  dim3 gridu(g.nit, g.njt, g.nkc_u);
   SolveState s0{};
   s0.epscg = 0.0;
   s0.ncgmax = 0x7fffffff;
@@ -1232,8 +1305,8 @@ int Solver::time_kernels(int reps, double ms[2], double bytes[2]) {
   ua.s1z_part = d_s1z;
   ua.st = d_state;
   ua.partials = d_partials;
-  k_update<UPD_BDOTB, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
-  k_update<UPD_INIT, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
+  k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  k_update<UPD_INIT, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   CK(cudaGetLastError());
   cudaEvent_t e[3];
   for (auto &x : e) CK(cudaEventCreate(&x));
@@ -1260,7 +1333,7 @@ int Solver::time_kernels(int reps, double ms[2], double bytes[2]) {
     CK(cudaEventRecord(e[0], stream));
     k_stencil<MODE_PCG><<<grid, NTHR, StageLayout<MODE_PCG>::smem, stream>>>(mp, g, m, sa);
     CK(cudaEventRecord(e[1], stream));
-    k_update<UPD_ITER, false><<<grid, NTHR, 0, stream>>>(g, m, ua);
+    k_update<UPD_ITER, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
     CK(cudaEventRecord(e[2], stream));
     CK(cudaEventSynchronize(e[2]));
     float a = 0.f, b = 0.f;

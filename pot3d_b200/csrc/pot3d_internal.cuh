@@ -36,8 +36,10 @@ struct Geo {
   int nr, nt, np;
   int nrm2, ntm2, npm2;
   int NRP;      // padded radial line length
-  int tk;       // k-planes per block in tiled kernels
-  int nkc;      // number of k chunks (gridDim.z)
+  int tk;       // k-planes per block of the stencil kernel
+  int nkc;      // number of k chunks of the stencil kernel (gridDim.z)
+  int tk_u;     // k-planes per block of the update kernels
+  int nkc_u;    // number of k chunks of the update kernels
   int nit;      // number of i tiles (gridDim.x)
   int njt;      // number of j tiles (gridDim.y)
   long long Np; // padded vector length
