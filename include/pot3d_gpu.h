@@ -164,6 +164,23 @@ int pot3d_gpu_precond_diag(pot3d_gpu_solver *s, float *d, float *dinv);
  * update: x, p, r, Ap read, x, r written; 8 B each per unknown). */
 int pot3d_gpu_time_kernels(pot3d_gpu_solver *s, int reps, double ms[2], double bytes[2]);
 
+/* Magnetic energies like pot3d_gpu_energy, for callers that cannot allocate
+ * device memory (their memory is owned by another allocator, or they run
+ * while a stream is captured into a graph).  No counterpart in the
+ * reference.  All arrays are caller-owned DEVICE arrays, 0-based, with the
+ * lengths of pot3d_mesh_t; phi is (nr,nt,np) column-major; w receives
+ * {W_r, W_t, W_p} on the device, asynchronously on `stream` (a cudaStream_t,
+ * NULL for the default stream).  Scratch is a fixed file-scope device array
+ * of 8192 phi planes (3 doubles each): np-2 > 8192 is rejected with
+ * POT3D_ERR_ARG.  The library calls no cudaMalloc for it; the first call on
+ * a device looks up the array's device address, so make it before any
+ * stream capture.  Calls share that scratch: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int pot3d_gpu_energy_noalloc(int nr, int nt, int np, const double *rh, const double *dr,
+                             const double *drh, const double *dt, const double *dth,
+                             const double *sth, const double *dp, const double *dph,
+                             const double *phi, double *w, void *stream);
+
 /* Message for the most recent failing call on this thread. */
 const char *pot3d_gpu_last_error(void);
 

@@ -1,0 +1,60 @@
+"""pot3d_gpu_energy_noalloc: the energy diagnostic for callers that cannot
+allocate device memory (their memory belongs to another allocator, or they
+run during stream capture).  It must give the same energies as
+pot3d_gpu_energy, call after call, while the library allocates nothing for
+it.  This file is collected last so a stop at the first failure has already
+run every other test.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from pot3d_b200 import _lib, host
+from pot3d_b200.solver import Pot3dSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def _fn():
+    L = _lib.lib()
+    f = L.pot3d_gpu_energy_noalloc
+    f.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 10 + [C.c_void_p]
+    f.restype = C.c_int
+    return f
+
+
+def test_energy_noalloc_matches_energy_on_two_calls(cuda):
+    import torch
+
+    mesh = host.make_mesh(37, 30, 26)
+    tn, pn, fi = host.synthetic_br(4, 15, 4, 30, 26)
+    br0 = host.br0_from_map(mesh, tn, pn, fi)
+    rng = np.random.default_rng(11)
+    with Pot3dSolver(mesh, br0) as s:
+        phis = [s.finalize_phi(rng.standard_normal(s.N)) for _ in range(2)]
+        refs = [s.energy(p) for p in phis]
+    dev = {k: torch.tensor(getattr(mesh, k), device=cuda) for k in ("rh", "dr", "drh", "dt", "dth", "sth", "dp", "dph")}
+    f = _fn()
+    names = ("rh", "dr", "drh", "dt", "dth", "sth", "dp", "dph")
+    phs = [torch.tensor(np.asfortranarray(p).ravel(order="F"), device=cuda) for p in phis]
+    ws = [torch.full((3,), float("nan"), dtype=torch.float64, device=cuda) for _ in phis]
+    torch.cuda.synchronize()
+    free = []
+    for ph, w, ref in zip(phs, ws, refs):
+        rc = f(mesh.nr, mesh.nt, mesh.np, *[C.c_void_p(dev[k].data_ptr()) for k in names],
+               C.c_void_p(ph.data_ptr()), C.c_void_p(w.data_ptr()), None)
+        assert rc == 0, _lib.lib().pot3d_gpu_last_error()
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
+        got = w.cpu().numpy()
+        assert np.all(np.abs(got - ref) <= 1e-12 * np.abs(ref)), (got, ref)
+    assert free[1] >= free[0]  # the second call took no device memory
+
+
+def test_energy_noalloc_rejects_oversized_mesh(cuda):
+    f = _fn()
+    one = C.c_void_p(1)
+    rc = f(10, 10, 8192 + 3, *([one] * 10), None)
+    assert rc == 1
+    assert b"exceeds the scratch limit" in _lib.lib().pot3d_gpu_last_error()
