@@ -923,7 +923,9 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   g.nit = (g.nrm2 + TI - 1) / TI;
   g.njt = (g.ntm2 + TJ - 1) / TJ;
 
-  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  // A blocking stream: ordered with the legacy default stream, where callers
+  // (the Fortran host, torch) produce their device arrays and cudaMemset runs.
+  CK(cudaStreamCreate(&stream));
   {
     int e;
     if ((e = set_stencil_smem<MODE_AX>()) || (e = set_stencil_smem<MODE_PCG>()) || (e = set_stencil_smem<MODE_PCGZ>()))
