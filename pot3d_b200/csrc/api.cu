@@ -93,7 +93,7 @@ static int solve_common(pot3d_gpu_solver *h, const double *x_dev, const double *
   int ie = 1;
   pot3d_solve_info_t inf{};
   if (s.precision == POT3D_FP32_REFINED)
-    st = pot3d::mixed_solve(&s, zero_guess, ncgmax, epscg, &ie, &inf);
+    st = s.mixed_solve(zero_guess, ncgmax, epscg, &ie, &inf);
   else
     st = s.cgsolve_padded(zero_guess, ncgmax, epscg, &ie, &inf);
   if (st) return st;

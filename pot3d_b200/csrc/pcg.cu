@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <type_traits>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -154,7 +155,7 @@ __device__ __forceinline__ double apply_fac(const PtFac &f, double dpim, double 
 //   j=nt ghost = 2*S1(i) - x(i,ntm1,k), S1 the ring mean of x at j=ntm1
 //   k    periodic wrap (seam_hhh, src/pot3d.F90:5746-5758)
 // ============================================================================
-enum { MODE_AX = 0, MODE_PCG = 1, MODE_PCGZ = 2 };
+enum { MODE_AX = 0, MODE_PCG = 1, MODE_PCGZ = 2, MODE_PCG32 = 3 };
 
 struct StencilArgs {
   const double *x;          // AX input
@@ -165,6 +166,10 @@ struct StencilArgs {
   const float *z32;         // PCGZ
   double *p_new;            // PCG out
   double *q;                // PCG out
+  const float *p_old32;     // PCG32: FP32 inner vectors
+  const float *r32;
+  float *p_new32;
+  float *q32;
   const double *s1_direct;  // AX: S1(e), length NRP
   const double *s1z_part;   // PCG: [nkc][NRP] ring partial sums of z
   double *s1p;              // PCG: [2][NRP] ring sums of p (parity buffers)
@@ -204,6 +209,10 @@ template <>
 struct StageCfg<MODE_PCGZ> {
   static constexpr int n64 = 1, n32 = 1;
 };
+template <>
+struct StageCfg<MODE_PCG32> {
+  static constexpr int n64 = 0, n32 = 3;
+};
 template <int MODE>
 struct StageLayout {
   static constexpr int n64 = StageCfg<MODE>::n64, n32 = StageCfg<MODE>::n32;
@@ -216,13 +225,43 @@ struct StageLayout {
 // Tensor maps of the stage inputs: m64[0] = x | p_old, m64[1] = r, m32 = a_i | z.
 struct StencilMaps {
   CUtensorMap m64[2];
-  CUtensorMap m32;
+  CUtensorMap m32[3];
 };
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
+template <typename T>
+__device__ __forceinline__ T apply_fac_t(const PtFac &f, T dpim, T dpip, T dphk, T xkm, T xjm, T xim, T xc, T xip,
+                                         T xjp, T xkp) {
+  if constexpr (sizeof(T) == 8) {
+    return apply_fac(f, dpim, dpip, dphk, xkm, xjm, xim, xc, xip, xjp, xkp);
+  } else {
+    const float g1 = (float)f.g1, g2 = (float)f.g2, g3 = (float)f.g3, g5 = (float)f.g5, g6 = (float)f.g6,
+                gs = (float)f.gs;
+    const float a4 = fmaf(g1, dpim + dpip, gs * dphk);
+    const float tk = fmaf(dpim, xkm, dpip * xkp);
+    const float tr = fmaf(g3, xim, g5 * xip);
+    const float tt = fmaf(g2, xjm, g6 * xjp);
+    const float off = fmaf(g1, tk, dphk * (tr + tt));
+    return fmaf(a4, xc, -off);
+  }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(NTHR, 2)
     k_stencil(const __grid_constant__ StencilMaps maps, Geo g, DevMesh m, StencilArgs a) {
   using L = StageLayout<MODE>;
+  using T = typename std::conditional<MODE == MODE_PCG32, float, double>::type;
+  using T2 = typename Vec2<T>::type;
   extern __shared__ __align__(1024) unsigned char dyn[];
   __shared__ __align__(8) uint64_t bar[S_STAGES];
   __shared__ double red[NTHR / 32];
@@ -239,7 +278,7 @@ __global__ void __launch_bounds__(NTHR, 2)
   }
   double *kfac = reinterpret_cast<double *>(dyn + L::kfac_off);  // [tk][3]
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~uintptr_t(127));
-  double *pn_ring = reinterpret_cast<double *>(base + S_STAGES * L::bytes);  // [PN_SLOTS][BOX_Y][BOX64_X]
+  T *pn_ring = reinterpret_cast<T *>(base + S_STAGES * L::bytes);  // [PN_SLOTS][BOX_Y][BOX64_X]
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -259,9 +298,9 @@ __global__ void __launch_bounds__(NTHR, 2)
     abort_flag = 0;
     for (int s = 0; s < S_STAGES; s++) mbar_init(&bar[s], 1);
     mbar_init_fence();
-    tma_prefetch_desc(&maps.m64[0]);
+    if (L::n64 > 0) tma_prefetch_desc(&maps.m64[0]);
     if (L::n64 > 1) tma_prefetch_desc(&maps.m64[1]);
-    if (L::n32 > 0) tma_prefetch_desc(&maps.m32);
+    for (int q = 0; q < L::n32; q++) tma_prefetch_desc(&maps.m32[q]);
   }
   if (tid < TI) s1sh[tid] = 0.0;
   __syncthreads();
@@ -274,9 +313,9 @@ __global__ void __launch_bounds__(NTHR, 2)
     const int s = local % S_STAGES;
     unsigned char *st = base + s * L::bytes;
     mbar_expect_tx(&bar[s], L::tx);
-    tma_load_3d(st, &maps.m64[0], ib - 2, j0 - 1, kk, &bar[s]);
-    if (L::n64 > 1) tma_load_3d(st + TILE64_PITCH, &maps.m64[1], ib - 2, j0 - 1, kk, &bar[s]);
-    if (L::n32 > 0) tma_load_3d(st + L::n64 * TILE64_PITCH, &maps.m32, ib - 4, j0 - 1, kk, &bar[s]);
+    for (int q = 0; q < L::n64; q++) tma_load_3d(st + q * TILE64_PITCH, &maps.m64[q], ib - 2, j0 - 1, kk, &bar[s]);
+    for (int q = 0; q < L::n32; q++)
+      tma_load_3d(st + L::n64 * TILE64_PITCH + q * TILE32_PITCH, &maps.m32[q], ib - 4, j0 - 1, kk, &bar[s]);
   };
   int issued = 0;
   if (tid == 0) {
@@ -317,9 +356,16 @@ __global__ void __launch_bounds__(NTHR, 2)
   double dot = 0.0;
 
   // p_new at (row, col) of the stage tile; col counts FP64 columns.
-  auto pnew_at = [&](const unsigned char *st, int row, int col) -> double {
+  const float betaf = (float)beta;
+  auto pnew_at = [&](const unsigned char *st, int row, int col) -> T {
     const double *t0 = reinterpret_cast<const double *>(st);
-    if (MODE == MODE_AX) {
+    if constexpr (MODE == MODE_PCG32) {
+      const float *f0 = reinterpret_cast<const float *>(st);
+      const float *f1 = reinterpret_cast<const float *>(st + TILE32_PITCH);
+      const float *f2 = reinterpret_cast<const float *>(st + 2 * TILE32_PITCH);
+      const int c = row * BOX32_X + col + 2;
+      return fmaf(betaf, f0[c], f2[c] * f1[c]);
+    } else if (MODE == MODE_AX) {
       return t0[row * BOX64_X + col];
     } else if (MODE == MODE_PCG) {
       const double *t1 = reinterpret_cast<const double *>(st + TILE64_PITCH);
@@ -337,7 +383,7 @@ __global__ void __launch_bounds__(NTHR, 2)
     const uint32_t parity = (local / S_STAGES) & 1;
     if (!mbar_wait(&bar[s], parity, WAIT_LIMIT)) abort_flag = 1;
     const unsigned char *st = base + s * L::bytes;
-    double *slot = pn_ring + (local % PN_SLOTS) * (BOX_Y * BOX64_X);
+    T *slot = pn_ring + (local % PN_SLOTS) * (BOX_Y * BOX64_X);
     // own pair
     {
       const int col = 2 + el;
@@ -364,36 +410,46 @@ __global__ void __launch_bounds__(NTHR, 2)
     }
     if (local >= 2 && v0) {
       const int kk = p_first + local - 1;  // plane whose stencil is now complete
-      const double *sc = pn_ring + ((local - 1) % PN_SLOTS) * (BOX_Y * BOX64_X);
-      const double *sm = pn_ring + ((local - 2) % PN_SLOTS) * (BOX_Y * BOX64_X);
-      const double *sp = slot;
+      const T *sc = pn_ring + ((local - 1) % PN_SLOTS) * (BOX_Y * BOX64_X);
+      const T *sm = pn_ring + ((local - 2) % PN_SLOTS) * (BOX_Y * BOX64_X);
+      const T *sp = slot;
       const int kq = kk - k0;
-      const double dpim = kfac[3 * kq], dpip = kfac[3 * kq + 1], dphk = kfac[3 * kq + 2];
+      const T dpim = (T)kfac[3 * kq], dpip = (T)kfac[3 * kq + 1], dphk = (T)kfac[3 * kq + 2];
       const int col = 2 + el;
-      const double *rowc = sc + (w + 1) * BOX64_X;
-      const double2 xc = *reinterpret_cast<const double2 *>(rowc + col);
-      const double2 xm = *reinterpret_cast<const double2 *>(sm + (w + 1) * BOX64_X + col);
-      const double2 xn = *reinterpret_cast<const double2 *>(sp + (w + 1) * BOX64_X + col);
-      const double2 xjm2 = *reinterpret_cast<const double2 *>(sc + w * BOX64_X + col);
-      const double2 xjp2 = *reinterpret_cast<const double2 *>(sc + (w + 2) * BOX64_X + col);
-      const double xim = (e0 == 0) ? xc.x : rowc[col - 1];
-      const double xip = (e0 == g.nrm2 - 1) ? pm * xc.x : xc.y;
-      const double xjm = (jj == 0) ? 0.0 : xjm2.x;
-      const double xjp = south ? 2.0 * s1a - xc.x : xjp2.x;
-      const double y = apply_fac(f0, dpim, dpip, dphk, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
-      double y1 = 0.0;
+      const T *rowc = sc + (w + 1) * BOX64_X;
+      const T2 xc = *reinterpret_cast<const T2 *>(rowc + col);
+      const T2 xm = *reinterpret_cast<const T2 *>(sm + (w + 1) * BOX64_X + col);
+      const T2 xn = *reinterpret_cast<const T2 *>(sp + (w + 1) * BOX64_X + col);
+      const T2 xjm2 = *reinterpret_cast<const T2 *>(sc + w * BOX64_X + col);
+      const T2 xjp2 = *reinterpret_cast<const T2 *>(sc + (w + 2) * BOX64_X + col);
+      const T pmT = (T)pm, two = (T)2;
+      const T xim = (e0 == 0) ? xc.x : rowc[col - 1];
+      const T xip = (e0 == g.nrm2 - 1) ? pmT * xc.x : xc.y;
+      const T xjm = (jj == 0) ? (T)0 : xjm2.x;
+      const T xjp = south ? two * (T)s1a - xc.x : xjp2.x;
+      const T y = apply_fac_t<T>(f0, dpim, dpip, dphk, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
+      T y1 = (T)0;
       if (v1) {
-        const double xip1 = (e0 + 1 == g.nrm2 - 1) ? pm * xc.y : rowc[col + 2];
-        const double xjm1 = (jj == 0) ? 0.0 : xjm2.y;
-        const double xjp1 = south ? 2.0 * s1b - xc.y : xjp2.y;
-        y1 = apply_fac(f1, dpim, dpip, dphk, xm.y, xjm1, xc.x, xc.y, xip1, xjp1, xn.y);
+        const T xip1 = (e0 + 1 == g.nrm2 - 1) ? pmT * xc.y : rowc[col + 2];
+        const T xjm1 = (jj == 0) ? (T)0 : xjm2.y;
+        const T xjp1 = south ? two * (T)s1b - xc.y : xjp2.y;
+        y1 = apply_fac_t<T>(f1, dpim, dpip, dphk, xm.y, xjm1, xc.x, xc.y, xip1, xjp1, xn.y);
       }
       const long long id = g.idx(e0, jj, kk);
-      const double2 yv = make_double2(y, y1);
-      if (MODE == MODE_AX) {
+      T2 yv;
+      yv.x = y;
+      yv.y = y1;
+      T2 own;
+      own.x = xc.x;
+      own.y = v1 ? xc.y : (T)0;
+      if constexpr (MODE == MODE_AX) {
         *reinterpret_cast<double2 *>(a.y + id) = yv;
+      } else if constexpr (MODE == MODE_PCG32) {
+        *reinterpret_cast<float2 *>(a.q32 + id) = yv;
+        *reinterpret_cast<float2 *>(a.p_new32 + id) = own;
+        dot = fma((double)own.x, (double)y, dot);
+        dot = fma((double)own.y, (double)y1, dot);
       } else {
-        const double2 own = make_double2(xc.x, v1 ? xc.y : 0.0);
         *reinterpret_cast<double2 *>(a.q + id) = yv;
         *reinterpret_cast<double2 *>(a.p_new + id) = own;
         dot = fma(own.x, y, dot);
@@ -565,6 +621,140 @@ __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__r
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x)
     r32[t] = (float)r[t];
+}
+
+// ============================================================================
+// FP32-inner / FP64-refined PCG.  Inner iterations keep p, r, q and the
+// solution correction xs in FP32 and do the stencil and the preconditioner
+// in FP32; every dot product is accumulated in FP64 and alpha, beta stay
+// FP64 on the device.  A reliable update folds xs into the FP64 solution,
+// recomputes the true residual b - A x in FP64 and its preconditioned norm
+// (the reference's epsn), and restarts the recurrence residual from it while
+// keeping the search direction.  Convergence is decided on that true epsn.
+// ============================================================================
+struct Update32Args {
+  float *xs;
+  const float *p;
+  float *r;
+  const float *q;
+  const float *ai;
+  double *s1z_part;
+  SolveState *st;
+  double *partials;
+};
+enum { U32_ITER = 0, U32_RESTART = 1 };
+
+template <int KIND>
+__global__ void __launch_bounds__(NTHR) k_update32(Geo g, DevMesh m, Update32Args a) {
+  __shared__ double red[NTHR / 32];
+  const volatile SolveState *vs = a.st;
+  if (KIND == U32_ITER && vs->status != ST_RUNNING) return;
+  const float alpha = (KIND == U32_ITER) ? (float)vs->alpha : 0.0f;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int e0 = blockIdx.x * TI + 2 * lane;
+  const int jj = blockIdx.y * TJ + w;
+  const int k0 = blockIdx.z * g.tk_u;
+  const int k1 = min(k0 + g.tk_u, g.npm2);
+  const bool v0 = jj < g.ntm2 && e0 < g.nrm2;
+  const bool v1 = v0 && e0 + 1 < g.nrm2;
+  const bool south = v0 && jj == g.ntm2 - 1;
+  double rz = 0.0, s1a = 0.0, s1b = 0.0;
+  if (v0) {
+#pragma unroll 4
+    for (int kk = k0; kk < k1; kk++) {
+      const long long id = g.idx(e0, jj, kk);
+      float2 rv = *reinterpret_cast<const float2 *>(a.r + id);
+      if (KIND == U32_ITER) {
+        float2 xv = *reinterpret_cast<const float2 *>(a.xs + id);
+        const float2 pv = __ldg(reinterpret_cast<const float2 *>(a.p + id));
+        const float2 qv = __ldg(reinterpret_cast<const float2 *>(a.q + id));
+        xv.x = fmaf(alpha, pv.x, xv.x);
+        xv.y = fmaf(alpha, pv.y, xv.y);
+        rv.x = fmaf(-alpha, qv.x, rv.x);
+        rv.y = fmaf(-alpha, qv.y, rv.y);
+        *reinterpret_cast<float2 *>(a.xs + id) = xv;
+        *reinterpret_cast<float2 *>(a.r + id) = rv;
+      }
+      const float2 av = __ldg(reinterpret_cast<const float2 *>(a.ai + id));
+      const float zx = av.x * rv.x, zy = v1 ? av.y * rv.y : 0.0f;
+      rz = fma((double)rv.x, (double)zx, rz);
+      rz = fma((double)rv.y, (double)zy, rz);
+      if (south) {
+        const double wk = m.dph[kk + 2];
+        s1a += __dmul_rn((double)zx, wk) * m.pl_i;
+        s1b += __dmul_rn((double)zy, wk) * m.pl_i;
+      }
+    }
+  }
+  if (south) {
+    a.s1z_part[(long long)blockIdx.z * g.NRP + e0] = s1a;
+    a.s1z_part[(long long)blockIdx.z * g.NRP + e0 + 1] = v1 ? s1b : 0.0;
+  }
+  const double bs = block_sum<NTHR>(rz, red);
+  double total;
+  const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+  if (last_block_sum<NTHR>(bs, a.partials, &a.st->cnt_b, nb, &total, red)) {
+    if (threadIdx.x == 0) {
+      SolveState *s = a.st;
+      if (KIND == U32_ITER) {
+        s->rho_old = s->rho;
+        s->rho = total;
+        s->ncg = s->ncg + 1;
+        const double epssq = total / s->bdotb;
+        const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
+        s->epsn = epsn;
+        if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
+        if (!isfinite(epsn)) {
+          s->status = ST_BREAKDOWN;
+        } else if (epsn < s->epscg) {
+          s->status = ST_CONVERGED;  // candidate: confirmed by the FP64 residual
+        } else if (s->ncg >= s->ncgmax) {
+          s->status = ST_MAXIT;
+        }
+        s->beta = total / s->rho_old;
+      } else {
+        // restart from the true residual: rho <- r.z, beta continues the
+        // recurrence with the previous rho (zero on the first start).
+        s->rho = total;
+        s->beta = (s->rho_old > 0.0) ? total / s->rho_old : 0.0;
+        const double epssq = s->rho_true / s->bdotb;
+        const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
+        s->epsn = epsn;
+        if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
+        s->status = (epsn < s->epscg) ? ST_CONVERGED : (s->ncg >= s->ncgmax ? ST_MAXIT : ST_RUNNING);
+      }
+    }
+  }
+}
+
+// x += (double)xs; xs = 0   (the FP64 solution update of a reliable update)
+__global__ void k_fold(long long n, double *__restrict__ x, float *__restrict__ xs) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    x[t] += (double)xs[t];
+    xs[t] = 0.0f;
+  }
+}
+
+// r = b - q (FP64 true residual), r32 = (float)r, and r.(a_i r) in FP64.
+__global__ void __launch_bounds__(NTHR) k_true_resid(long long n, const double *__restrict__ b,
+                                                     const double *__restrict__ q, const float *__restrict__ ai,
+                                                     double *__restrict__ r, float *__restrict__ r32, SolveState *st,
+                                                     double *partials) {
+  __shared__ double red[NTHR / 32];
+  double acc = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const double v = b[t] - q[t];
+    r[t] = v;
+    r32[t] = (float)v;
+    acc = fma(v, (double)ai[t] * v, acc);
+  }
+  const double bs = block_sum<NTHR>(acc, red);
+  double total;
+  if (last_block_sum<NTHR>(bs, partials, &st->cnt_c, gridDim.x, &total, red)) {
+    if (threadIdx.x == 0) st->rho_true = total;
+  }
 }
 
 // ============================================================================
@@ -885,7 +1075,7 @@ Solver::~Solver() {
   if (stream) cudaStreamSynchronize(stream);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (dilu) dilu_destroy(this);
-  if (mixed) mixed_destroy(this);
+  if (graph32_exec) cudaGraphExecDestroy(graph32_exec);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   for (void *p : allocs) cudaFree(p);
@@ -928,7 +1118,8 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   CK(cudaStreamCreate(&stream));
   {
     int e;
-    if ((e = set_stencil_smem<MODE_AX>()) || (e = set_stencil_smem<MODE_PCG>()) || (e = set_stencil_smem<MODE_PCGZ>()))
+    if ((e = set_stencil_smem<MODE_AX>()) || (e = set_stencil_smem<MODE_PCG>()) ||
+        (e = set_stencil_smem<MODE_PCGZ>()) || (e = set_stencil_smem<MODE_PCG32>()))
       return e;
   }
   // k-chunking by a wave model: the grid is (i tiles, j tiles, k chunks);
@@ -1029,7 +1220,14 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
     if ((st = dilu_setup(this))) return st;
   }
   if (precision == POT3D_FP32_REFINED) {
-    if ((st = mixed_setup(this))) return st;
+    if (ifprec == 2) {
+      pot3d_set_error("the FP32-refined solve supports ifprec 0 and 1");
+      return POT3D_ERR_ARG;
+    }
+    const size_t fb = sizeof(float) * (size_t)g.Np;
+    if ((st = alloc((void **)&m_p32a, fb)) || (st = alloc((void **)&m_p32b, fb)) || (st = alloc((void **)&m_r32, fb)) ||
+        (st = alloc((void **)&m_q32, fb)) || (st = alloc((void **)&m_xs32, fb)))
+      return st;
   }
   CK(cudaStreamSynchronize(stream));
   return POT3D_OK;
@@ -1051,7 +1249,7 @@ int Solver::ax_padded(const double *x, double *y) {
   int st;
   if ((st = tensor_map(x, true, &mp.m64[0]))) return st;
   mp.m64[1] = mp.m64[0];
-  mp.m32 = mp.m64[0];
+  mp.m32[0] = mp.m32[1] = mp.m32[2] = mp.m64[0];
   dim3 grid(g.nit, g.njt, g.nkc);
   dim3 gridu(g.nit, g.njt, g.nkc_u);
   k_stencil<MODE_AX><<<grid, NTHR, StageLayout<MODE_AX>::smem, stream>>>(mp, g, m, a);
@@ -1116,7 +1314,7 @@ int Solver::launch_iteration() {
   if (ifprec == 2) {
     sa.z32 = dilu_z32(this);
     mp.m64[1] = mp.m64[0];
-    if ((stm = tensor_map(sa.z32, false, &mp.m32))) return stm;
+    if ((stm = tensor_map(sa.z32, false, &mp.m32[0]))) return stm;
     k_stencil<MODE_PCGZ><<<grid, NTHR, StageLayout<MODE_PCGZ>::smem, stream>>>(mp, g, m, sa);
     ua.r32 = dilu_r32(this);
     k_update_r32<<<grid1d(g.Np / 2), NTHR, 0, stream>>>(g, ua);
@@ -1126,7 +1324,7 @@ int Solver::launch_iteration() {
     k_update<UPD_ZDOT, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   } else {
     if ((stm = tensor_map(d_r, true, &mp.m64[1]))) return stm;
-    if ((stm = tensor_map(d_ai, false, &mp.m32))) return stm;
+    if ((stm = tensor_map(d_ai, false, &mp.m32[0]))) return stm;
     k_stencil<MODE_PCG><<<grid, NTHR, StageLayout<MODE_PCG>::smem, stream>>>(mp, g, m, sa);
     k_update<UPD_ITER, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   }
@@ -1330,7 +1528,7 @@ int Solver::time_kernels(int reps, double ms[2], double bytes[2]) {
     StencilMaps mp;
     int stm;
     if ((stm = tensor_map(p_cur, true, &mp.m64[0])) || (stm = tensor_map(d_r, true, &mp.m64[1])) ||
-        (stm = tensor_map(d_ai, false, &mp.m32)))
+        (stm = tensor_map(d_ai, false, &mp.m32[0])))
       return stm;
     CK(cudaEventRecord(e[0], stream));
     k_stencil<MODE_PCG><<<grid, NTHR, StageLayout<MODE_PCG>::smem, stream>>>(mp, g, m, sa);
@@ -1393,6 +1591,183 @@ int Solver::energy_dev(const double *phi, double w[3]) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(w, d_scalar, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
+  return POT3D_OK;
+}
+
+}  // namespace pot3d
+
+namespace pot3d {
+
+// One FP32 inner iteration: stencil+dot, update+dot.
+int Solver::launch_iteration32() {
+  dim3 grid(g.nit, g.njt, g.nkc);
+  dim3 gridu(g.nit, g.njt, g.nkc_u);
+  StencilArgs sa{};
+  sa.p_old32 = p32_cur;
+  sa.p_new32 = p32_nxt;
+  sa.r32 = m_r32;
+  sa.q32 = m_q32;
+  sa.s1z_part = d_s1z;
+  sa.s1p = d_s1p;
+  sa.st = d_state;
+  sa.partials = d_partials;
+  StencilMaps mp;
+  int stm;
+  if ((stm = tensor_map(p32_cur, false, &mp.m32[0])) || (stm = tensor_map(m_r32, false, &mp.m32[1])) ||
+      (stm = tensor_map(d_ai, false, &mp.m32[2])))
+    return stm;
+  mp.m64[0] = mp.m64[1] = mp.m32[0];
+  k_stencil<MODE_PCG32><<<grid, NTHR, StageLayout<MODE_PCG32>::smem, stream>>>(mp, g, m, sa);
+  Update32Args ua{};
+  ua.xs = m_xs32;
+  ua.p = p32_nxt;
+  ua.r = m_r32;
+  ua.q = m_q32;
+  ua.ai = d_ai;
+  ua.s1z_part = d_s1z;
+  ua.st = d_state;
+  ua.partials = d_partials;
+  k_update32<U32_ITER><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  std::swap(p32_cur, p32_nxt);
+  return pot3d_cuda_status(cudaGetLastError(), "launch_iteration32");
+}
+
+// Reliable update: x += xs, r = b - A x in FP64, epsn of the true residual,
+// restart of the FP32 recurrence residual from it.
+int Solver::reliable_update(bool fold) {
+  int st;
+  if (fold) k_fold<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_x, m_xs32);
+  if ((st = ax_padded(d_x, d_q))) return st;
+  k_true_resid<<<148 * 4, NTHR, 0, stream>>>(g.Np, d_b, d_q, d_ai, d_r, m_r32, d_state, d_partials + 4096);
+  dim3 gridu(g.nit, g.njt, g.nkc_u);
+  Update32Args ua{};
+  ua.xs = m_xs32;
+  ua.p = p32_cur;
+  ua.r = m_r32;
+  ua.q = m_q32;
+  ua.ai = d_ai;
+  ua.s1z_part = d_s1z;
+  ua.st = d_state;
+  ua.partials = d_partials;
+  k_update32<U32_RESTART><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  launches += (fold ? 1 : 0) + 4;
+  return pot3d_cuda_status(cudaGetLastError(), "reliable_update");
+}
+
+int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info) {
+  (void)zero_guess;
+  dim3 gridu(g.nit, g.njt, g.nkc_u);
+  int st;
+  SolveState s0{};
+  s0.epscg = epscg;
+  s0.ncgmax = ncgmax;
+  s0.hist = d_hist;
+  s0.hist_cap = hist_cap;
+  CK(cudaMemcpyAsync(d_state, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, stream));
+  CK(cudaEventRecord(ev0, stream));
+  launches = 0;
+  p32_cur = m_p32a;
+  p32_nxt = m_p32b;
+  CK(cudaMemsetAsync(p32_cur, 0, sizeof(float) * g.Np, stream));
+  CK(cudaMemsetAsync(m_xs32, 0, sizeof(float) * g.Np, stream));
+  CK(cudaMemsetAsync(d_s1p, 0, sizeof(double) * 2 * g.NRP, stream));
+  // bdotb = b . M^-1 b in FP64 (src/pot3d.F90:4293-4298)
+  CK(cudaMemcpyAsync(d_r, d_b, sizeof(double) * g.Np, cudaMemcpyDeviceToDevice, stream));
+  UpdateArgs ub{};
+  ub.r = d_r;
+  ub.ai = d_ai;
+  ub.st = d_state;
+  ub.partials = d_partials;
+  k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, stream>>>(g, m, ub);
+  launches += 1;
+  CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (h_state->bdotb == 0.0) {
+    CK(cudaMemsetAsync(d_x, 0, sizeof(double) * g.Np, stream));
+    CK(cudaStreamSynchronize(stream));
+    *ierr = 0;
+    last_ncg = 0;
+    last_epsn = 0.0;
+    last_seconds = 0.0;
+    if (info) memset(info, 0, sizeof(*info));
+    return POT3D_OK;
+  }
+  if ((st = reliable_update(false))) return st;
+  int n_refine = 0;
+  CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  const double est_iter_s = 44.0 * (double)g.Np / 5.0e12 + 6e-6;
+  int U = (int)std::ceil(0.5e-3 / est_iter_s);
+  U = std::max(2, std::min(U, 32));
+  if (!graph32_exec || graph32_U != U) {
+    if (graph32_exec) cudaGraphExecDestroy(graph32_exec);
+    graph32_exec = nullptr;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int u = 0; u < 2 * U; u++) {
+      st = launch_iteration32();
+      if (st) {
+        cudaStreamEndCapture(stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+      }
+    }
+    CK(cudaStreamEndCapture(stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&graph32_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(e);
+    graph32_U = U;
+  }
+  const long long per_graph = 2LL * U;
+  double rho_ref = h_state->rho;
+  int last_seen = -1, stalls = 0;
+  while (h_state->status == ST_RUNNING) {
+    CK(cudaGraphLaunch(graph32_exec, stream));
+    launches += per_graph * 2;
+    CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    const int status = h_state->status;
+    if (status == ST_BREAKDOWN) break;
+    const bool refresh = status == ST_CONVERGED || status == ST_MAXIT || h_state->rho < refine_ratio * rho_ref;
+    if (refresh) {
+      if ((st = reliable_update(true))) return st;
+      n_refine++;
+      CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      rho_ref = h_state->rho;
+      if (status == ST_MAXIT && h_state->status == ST_RUNNING) h_state->status = ST_MAXIT;
+    }
+    if (h_state->ncg <= last_seen && h_state->status == ST_RUNNING) {
+      if (++stalls >= 3) {
+        pot3d_set_error("refined PCG state stopped advancing on the device");
+        return POT3D_ERR_TIMEOUT;
+      }
+    } else {
+      stalls = 0;
+    }
+    last_seen = h_state->ncg;
+  }
+  CK(cudaEventRecord(ev1, stream));
+  CK(cudaStreamSynchronize(stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  last_ncg = h_state->ncg;
+  last_epsn = h_state->epsn;
+  last_seconds = ms * 1e-3;
+  last_refine = n_refine;
+  if (h_state->status == ST_BREAKDOWN) {
+    pot3d_set_error("refined PCG breakdown (non-finite residual)");
+    return POT3D_ERR_BREAKDOWN;
+  }
+  *ierr = (h_state->status == ST_CONVERGED) ? 0 : 1;
+  if (info) {
+    info->ncg = last_ncg;
+    info->n_refine = n_refine;
+    info->epsn = last_epsn;
+    info->seconds = last_seconds;
+    info->true_resid = -1.0;
+    info->kernel_launches = launches;
+  }
   return POT3D_OK;
 }
 

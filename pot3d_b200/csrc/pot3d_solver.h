@@ -13,7 +13,6 @@
 namespace pot3d {
 
 struct DiluState;   // ILU(0) preconditioner (dilu.cu)
-struct MixedState;  // FP32-inner / FP64-refinement state (mixed.cu)
 
 struct Solver {
   Geo g{};
@@ -39,6 +38,16 @@ struct Solver {
   float *d_ai = nullptr;        // diagonal preconditioner (FP32, padded)
   double *p_cur = nullptr, *p_nxt = nullptr;
 
+  // FP32-refined mode
+  float *m_p32a = nullptr, *m_p32b = nullptr, *m_r32 = nullptr, *m_q32 = nullptr, *m_xs32 = nullptr;
+  float *p32_cur = nullptr, *p32_nxt = nullptr;
+  cudaGraphExec_t graph32_exec = nullptr;
+  int graph32_U = 0;
+  double refine_ratio = 1e-4;  // reliable update when r.z fell by this factor
+  int launch_iteration32();
+  int reliable_update(bool fold);
+  int mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info);
+
   cudaGraphExec_t graph_exec = nullptr;
   int graph_U = 0, graph_kind = -1;
 
@@ -51,7 +60,6 @@ struct Solver {
   int tensor_map(const void *ptr, bool fp64, CUtensorMap *out);
 
   DiluState *dilu = nullptr;
-  MixedState *mixed = nullptr;
 
   ~Solver();
   int alloc(void **p, size_t bytes);
@@ -84,10 +92,6 @@ int dilu_sweeps(Solver *s, bool check_status);
 int dilu_diag(Solver *s, float *d_host, float *dinv_host);
 int dilu_sweep_launches(Solver *s);
 
-// FP32-refined solve hooks (mixed.cu).
-int mixed_setup(Solver *s);
-void mixed_destroy(Solver *s);
-int mixed_solve(Solver *s, bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info);
 
 // Kernel launch helpers shared between translation units.
 int grid1d(long long n);

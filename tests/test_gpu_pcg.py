@@ -164,3 +164,33 @@ def test_kernel_timing_entry_point(cuda):
     with Pot3dSolver(mesh, br0) as s:
         ms, by = s.time_kernels(5)
         assert np.all(ms > 0) and by[0] == 32.0 * s.N and by[1] == 48.0 * s.N
+
+
+@pytest.mark.parametrize("dims,option", [((63, 91, 181), "ss"), ((37, 30, 26), "open")])
+def test_fp32_refined_solve_parity(cuda, dims, option):
+    """FP32 inner iterations with FP64 reliable updates reach the same
+    solution as the FP64 oracle at epscg 1e-11: convergence is decided on the
+    reference's epsn of the true FP64 residual."""
+    mesh, br0 = _case(*dims, option=option)
+    o = _oracle(mesh, br0, option=option)
+    ref = o.cgsolve(np.zeros(o.N), o.rhs(), epscg=1e-11)
+    phi_ref = o.finalize_phi(ref["x"])
+    w_ref = o.energy(phi_ref)
+    out = potfld(mesh, br0, option=option, precision="fp32_refined", epscg=1e-11)
+    assert out["ierr"] == 0 and out["epsn"] < 1e-11
+    assert out["n_refine"] >= 1
+    rel = np.linalg.norm(out["phi"] - phi_ref) / np.linalg.norm(phi_ref)
+    assert rel <= 1e-8, rel
+    assert np.all(np.abs(out["energy"] - w_ref) <= 1e-9 * np.abs(w_ref))
+    # the refined recurrence keeps the Krylov direction: few extra iterations
+    assert out["ncg"] <= 1.5 * ref["ncg"] + 20, (out["ncg"], ref["ncg"])
+
+
+def test_fp32_refined_true_residual_and_history(cuda):
+    mesh, br0 = _case(63, 91, 181)
+    out = potfld(mesh, br0, precision="fp32_refined", epscg=1e-9)
+    assert out["ierr"] == 0
+    # the returned r is the FP64 true residual b - A x of the returned x
+    assert out["true_resid"] < 1e-7
+    h = out["history"]
+    assert len(h) == out["ncg"] + 1 and h[-1] < 1e-9
