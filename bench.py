@@ -116,7 +116,7 @@ def build_case(name: str, rank: int = 0):
     w = dict(host.WORKLOADS[name])
     opt = w.pop("option", "ss")
     dnb = w.pop("do_not_balance_flux", False)
-    seed = w.pop("seed") + rank  # replicas solve different seeded maps
+    seed = replica_seed(w.pop("seed"), rank)
     mesh, br0 = host.pfss_case(w["nr"], w["nt"], w["np"], w["lmax"], w["nbip"], seed, option=opt,
                                do_not_balance_flux=dnb)
     return mesh, br0, opt, seed
@@ -145,25 +145,38 @@ def cpu_baseline(mesh, br0, option, ifprec, ncg_target, sample_iters):
             "seconds_per_iteration": per_it}
 
 
-def dist_init():
+def dist_init(backend=None):
+    """One process per GPU (or per CPU rank for gloo): env:// rendezvous."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
+        import datetime
+
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        kw = {}
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            kw["device_id"] = torch.device("cuda", local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600), **kw)
     return ws, rank, local
 
 
+def replica_seed(base_seed: int, rank: int) -> int:
+    """Replicas solve different seeded maps: rank r uses base_seed + r."""
+    return base_seed + rank
+
+
 def reduce_max(v: float, ws: int) -> float:
+    """Maximum over ranks (the job's time is its slowest replica)."""
     if ws == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
