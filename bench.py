@@ -226,6 +226,8 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="iteration count used to project the CPU sample (0: take it from a GPU solve)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-timing-only", action="store_true",
+                    help="time the stencil and update kernels once (used for ncu captures) and exit")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -240,6 +242,11 @@ def main():
     torch.cuda.set_device(local)
     mesh, br0, opt, seed = build_case(args.workload, rank)
     s = Pot3dSolver(mesh, br0, option=opt, ifprec=args.ifprec, precision=args.precision, device=local)
+    if args.kernel_timing_only:
+        ms, by = s.time_kernels(4)
+        print(json.dumps({"workload": args.workload, "ms": list(ms), "gbs": list(by / (ms * 1e-3) / 1e9)}))
+        s.close()
+        return 0
     b = s.rhs()
     N = s.N
     xt = torch.zeros(N, dtype=torch.float64, device="cuda")

@@ -124,6 +124,7 @@ def synthetic_br(seed: int, lmax: int, nbip: int, ntn: int, npn: int):
 WORKLOADS = {
     "pfss_63x91x181": dict(nr=63, nt=91, np=181, lmax=15, nbip=4, seed=1),
     "pfss_255x361x721": dict(nr=255, nt=361, np=721, lmax=40, nbip=20, seed=2),
+    "pfss_255x361x181": dict(nr=255, nt=361, np=181, lmax=40, nbip=20, seed=2),
     "pfss_127x181x361": dict(nr=127, nt=181, np=361, lmax=40, nbip=20, seed=1000),
     "open_511x721x1441": dict(nr=511, nt=721, np=1441, lmax=80, nbip=60, seed=7, option="open",
                               do_not_balance_flux=True),
