@@ -119,6 +119,12 @@ int pot3d_gpu_destroy(pot3d_gpu_solver *s);
 /* Number of unknowns N. */
 long pot3d_gpu_size(const pot3d_gpu_solver *s);
 
+/* Replace br0 (host, (nt,np) column-major) of a set-up solve, as set_flux
+ * would for a new boundary map (src/pot3d.F90:3754-3864), keeping the mesh,
+ * operator and preconditioner.  No counterpart in the reference, which
+ * solves one map per run. */
+int pot3d_gpu_set_br0(pot3d_gpu_solver *s, const double *br0);
+
 /* RHS by potfld's boundary trick, src/pot3d.F90:3937-3950 (host output). */
 int pot3d_gpu_rhs(pot3d_gpu_solver *s, double *rhs);
 

@@ -223,3 +223,18 @@ extern "C" int pot3d_gpu_time_kernels(pot3d_gpu_solver *h, int reps, double ms[2
   }
   return h->s.time_kernels(reps, ms, bytes);
 }
+
+extern "C" int pot3d_gpu_set_br0(pot3d_gpu_solver *h, const double *br0) {
+  int st;
+  if ((st = check_solver(h))) return st;
+  if (!br0) {
+    pot3d_set_error("pot3d_gpu_set_br0: null br0");
+    return POT3D_ERR_ARG;
+  }
+  Solver &s = h->s;
+  CKS(cudaMemcpyAsync(const_cast<double *>(s.m.br0), br0, sizeof(double) * (size_t)s.g.nt * s.g.np,
+                      cudaMemcpyHostToDevice, s.stream));
+  if ((st = s.rhs_padded(s.d_b))) return st;
+  CKS(cudaStreamSynchronize(s.stream));
+  return POT3D_OK;
+}

@@ -172,6 +172,24 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
   }
 }
 
+// x[b][p][0] = br0n[b][p]; x[b][p][1..3] = consts[p][0..2]; other channels 0.
+__global__ void k_inputs(const float *__restrict__ br0n, const float *__restrict__ consts, long long B, long long npos,
+                         __nv_bfloat16 *__restrict__ x) {
+  const long long n = B * npos * 64;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t & 63);
+    const long long bp = t >> 6;
+    const long long p = bp % npos;
+    float v = 0.0f;
+    if (c == 0)
+      v = br0n[bp];
+    else if (c < 4)
+      v = consts[p * 3 + (c - 1)];
+    x[t] = __float2bfloat16_rn(v);
+  }
+}
+
 int grid_for(long long n) {
   long long b = (n + 255) / 256;
   if (b > 148LL * 32) b = 148LL * 32;
@@ -244,4 +262,15 @@ extern "C" int pot3d_fno_adam(float *w, const float *g, float *m1, float *m2, vo
   k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(w, g, m1, m2, reinterpret_cast<__nv_bfloat16 *>(wb), n, lr, b1,
                                                          b2, eps, c1, c2);
   return pot3d_cuda_status(cudaGetLastError(), "pot3d_fno_adam");
+}
+
+extern "C" int pot3d_fno_inputs(const float *br0n, const float *consts, long long B, long long npos, void *x,
+                                void *stream) {
+  if (B < 1 || npos < 1) {
+    pot3d_set_error("pot3d_fno_inputs: bad sizes");
+    return POT3D_ERR_ARG;
+  }
+  k_inputs<<<grid_for(B * npos * 64), 256, 0, (cudaStream_t)stream>>>(br0n, consts, B, npos,
+                                                                     reinterpret_cast<__nv_bfloat16 *>(x));
+  return pot3d_cuda_status(cudaGetLastError(), "pot3d_fno_inputs");
 }

@@ -225,7 +225,7 @@ class FNO:
             cache["pre_lift"] = pre
         for l in range(self.nl):
             last = l == self.nl - 1
-            st = self._spectral(v, B) if not keep else self._spectral(v, B, cache, l)
+            st = self._spectral(v, B, cache, l)
             pre = tc_gemm(v, self.pb[f"W{l}"], bias=self.p[f"b{l}"])  # [M, 32]
             permute(st, (B, W_, g.nph, self.Pth), pre, (B, g.nph, g.nth, W_), (0, 2, 3, 1), add=True)
             if keep:

@@ -50,3 +50,17 @@ def test_fno_adam_steps_reduce_loss(cuda):
         losses.append(float(loss.mean().item()))
         model.adam_step(model.backward(grad_out), lr=3e-3)
     assert losses[-1] < 0.8 * losses[0], losses
+
+
+def test_fno_inference_equals_training_forward(cuda):
+    """The inference path (no activation cache) computes the same output as
+    the training path of the same weights, layer by layer."""
+    import torch
+    model, x, _ = _model_and_batch(seed=2)
+    for l in range(model.nl):  # distinct spectral weights per layer
+        model.p[f"R{l}"].mul_(1.0 + 0.5 * l)
+        model.pb[f"R{l}"] = model.p[f"R{l}"].to(torch.bfloat16).contiguous()
+    a = model.forward(x, keep=True).clone()
+    b = model.forward(x, keep=False)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
