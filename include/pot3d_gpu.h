@@ -187,6 +187,26 @@ int pot3d_gpu_energy_noalloc(int nr, int nt, int np, const double *rh, const dou
                              const double *sth, const double *dp, const double *dph,
                              const double *phi, double *w, void *stream);
 
+/* Batched solves: n independent cases (own mesh, br0 and pm_r1; ifprec=1,
+ * FP64 PCG), each tiled kernel launch covering the tiles of every unfinished
+ * case, with per-case convergence.  No counterpart in the reference, which
+ * solves one case per run.  tk: stencil planes per block (0 = the per-case
+ * default; see pot3d_gpu_batch_tune). */
+typedef struct pot3d_gpu_batch pot3d_gpu_batch;
+int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                           const double *pm_r1s, int tk, pot3d_gpu_batch **out);
+/* Autotuner: times `iters` batched iterations for each candidate planes per
+ * block, keeps the fastest (*best_tk; ms_out[c] = time of candidate c). */
+int pot3d_gpu_batch_tune(pot3d_gpu_batch *b, const int *candidates, int ncand, int iters, int *best_tk,
+                         float *ms_out);
+/* Solve all cases from x = 0 to epscg (ernorm's rule per case); ierr[i],
+ * info[i] per case; *seconds = device time of the whole batch. */
+int pot3d_gpu_batch_solve(pot3d_gpu_batch *b, int ncgmax, double epscg, int *ierr,
+                          pot3d_solve_info_t *info, double *seconds);
+/* Solution of case i (host, packed layout of length N_i). */
+int pot3d_gpu_batch_solution(pot3d_gpu_batch *b, int i, double *x);
+int pot3d_gpu_batch_destroy(pot3d_gpu_batch *b);
+
 /* Message for the most recent failing call on this thread. */
 const char *pot3d_gpu_last_error(void);
 

@@ -37,11 +37,6 @@ int pot3d_cuda_status(cudaError_t e, const char *where) {
 }
 extern "C" const char *pot3d_gpu_last_error(void) { return g_last_error.c_str(); }
 
-#define CK(call)                                                  \
-  do {                                                            \
-    int _st = pot3d_cuda_status((call), #call);                   \
-    if (_st != POT3D_OK) return _st;                              \
-  } while (0)
 
 // ============================================================================
 // Stencil coefficients (load_matrix_pot3d_solve, src/pot3d.F90:4590-4611).
@@ -257,8 +252,8 @@ __device__ __forceinline__ T apply_fac_t(const PtFac &f, T dpim, T dpip, T dphk,
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(NTHR, 2)
-    k_stencil(const __grid_constant__ StencilMaps maps, Geo g, DevMesh m, StencilArgs a) {
+__device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo &g, const DevMesh &m,
+                                             const StencilArgs &a, const int bx, const int by, const int bz) {
   using L = StageLayout<MODE>;
   using T = typename std::conditional<MODE == MODE_PCG32, float, double>::type;
   using T2 = typename Vec2<T>::type;
@@ -282,12 +277,12 @@ __global__ void __launch_bounds__(NTHR, 2)
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
-  const int ib = blockIdx.x * TI;
+  const int ib = bx * TI;
   const int el = 2 * lane;
   const int e0 = ib + el;
-  const int j0 = blockIdx.y * TJ;
+  const int j0 = by * TJ;
   const int jj = j0 + w;
-  const int k0 = blockIdx.z * g.tk;
+  const int k0 = bz * g.tk;
   const int k1 = min(k0 + g.tk, g.npm2);
   const bool rowv = jj < g.ntm2;
   const bool v0 = rowv && e0 < g.nrm2;
@@ -333,7 +328,7 @@ __global__ void __launch_bounds__(NTHR, 2)
       for (int c = 0; c < g.nkc_u; c++) sz += a.s1z_part[(long long)c * g.NRP + e];
       const double s = fma(beta, a.s1p[par * g.NRP + e], sz);
       s1sh[tid] = s;
-      if (blockIdx.z == 0) a.s1p[(par ^ 1) * g.NRP + e] = s;
+      if (bz == 0) a.s1p[(par ^ 1) * g.NRP + e] = s;
     }
   }
 
@@ -469,8 +464,9 @@ __global__ void __launch_bounds__(NTHR, 2)
   if (MODE != MODE_AX) {
     double bs = block_sum<NTHR>(dot, red);
     double total;
-    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-    if (last_block_sum<NTHR>(bs, a.partials, &a.st->cnt_a, nb, &total, red)) {
+    const unsigned nb = (unsigned)g.nit * g.njt * g.nkc;
+    const unsigned blin = (unsigned)bx + g.nit * ((unsigned)by + g.njt * (unsigned)bz);
+    if (last_block_sum_at<NTHR>(bs, a.partials, &a.st->cnt_a, nb, blin, &total, red)) {
       if (threadIdx.x == 0) {
         SolveState *s = a.st;
         s->pq = total;
@@ -484,6 +480,12 @@ __global__ void __launch_bounds__(NTHR, 2)
       }
     }
   }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NTHR, 2)
+    k_stencil(const __grid_constant__ StencilMaps maps, Geo g, DevMesh m, StencilArgs a) {
+  stencil_body<MODE>(maps, g, m, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ============================================================================
@@ -509,15 +511,16 @@ struct UpdateArgs {
 enum { UPD_ITER = 0, UPD_INIT = 1, UPD_BDOTB = 2, UPD_ZDOT = 3 };
 
 template <int KIND, bool ZIN>
-__global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a) {
+__device__ __forceinline__ void update_body(const Geo &g, const DevMesh &m, const UpdateArgs &a, const int bx,
+                                            const int by, const int bz) {
   __shared__ double red[NTHR / 32];
   const volatile SolveState *vs = a.st;
   if ((KIND == UPD_ITER || KIND == UPD_ZDOT) && vs->status != ST_RUNNING) return;
   const double alpha = (KIND == UPD_ITER) ? vs->alpha : 0.0;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int e0 = blockIdx.x * TI + 2 * lane;
-  const int jj = blockIdx.y * TJ + w;
-  const int k0 = blockIdx.z * g.tk_u;
+  const int e0 = bx * TI + 2 * lane;
+  const int jj = by * TJ + w;
+  const int k0 = bz * g.tk_u;
   const int k1 = min(k0 + g.tk_u, g.npm2);
   const bool v0 = jj < g.ntm2 && e0 < g.nrm2;
   const bool v1 = v0 && e0 + 1 < g.nrm2;
@@ -561,13 +564,14 @@ __global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a)
     }
   }
   if (south && KIND != UPD_BDOTB) {
-    a.s1z_part[(long long)blockIdx.z * g.NRP + e0] = s1a;
-    if (e0 + 1 < g.NRP) a.s1z_part[(long long)blockIdx.z * g.NRP + e0 + 1] = v1 ? s1b : 0.0;
+    a.s1z_part[(long long)bz * g.NRP + e0] = s1a;
+    if (e0 + 1 < g.NRP) a.s1z_part[(long long)bz * g.NRP + e0 + 1] = v1 ? s1b : 0.0;
   }
   const double bs = block_sum<NTHR>(rz, red);
   double total;
-  const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-  if (last_block_sum<NTHR>(bs, a.partials, &a.st->cnt_b, nb, &total, red)) {
+  const unsigned nb = (unsigned)g.nit * g.njt * g.nkc_u;
+  const unsigned blin = (unsigned)bx + g.nit * ((unsigned)by + g.njt * (unsigned)bz);
+  if (last_block_sum_at<NTHR>(bs, a.partials, &a.st->cnt_b, nb, blin, &total, red)) {
     if (threadIdx.x == 0) {
       SolveState *s = a.st;
       if (KIND == UPD_BDOTB) {
@@ -592,6 +596,11 @@ __global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a)
       }
     }
   }
+}
+
+template <int KIND, bool ZIN>
+__global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a) {
+  update_body<KIND, ZIN>(g, m, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ifprec=2 half of the update: x += alpha p ; r -= alpha q ; r32 = (float)r
@@ -1260,7 +1269,7 @@ int Solver::prec_padded(double *x) {
   if (ifprec == 2) {
     k_cast_r32<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, x, dilu_r32(this));
     int st = dilu_sweeps(this, false);
-    if (st) return st;
+    if (st || (st = dilu_status(this))) return st;
     // x = (double)z32
     k_widen<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, dilu_z32(this), x);
   } else {
@@ -1361,6 +1370,7 @@ int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr,
   ua.partials = d_partials;
   // bdotb = b . M^-1 b  (src/pot3d.F90:4293-4298)
   if (ifprec == 2) {
+    if ((st = dilu_reset(this))) return st;
     k_cast_r32<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_r, dilu_r32(this));
     if ((st = dilu_sweeps(this, false))) return st;
     ua.z32 = dilu_z32(this);
@@ -1403,7 +1413,7 @@ int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr,
   if (h_state->status == ST_RUNNING) {
     // Iterations run in CUDA graphs of 2U iterations; the host polls the
     // device status once per graph while the next graph is already queued.
-    const double est_iter_s = (ifprec == 2 ? 400.0 : 90.0) * (double)g.Np / 5.0e12 + 6e-6;
+    const double est_iter_s = (ifprec == 2 ? 140.0 : 90.0) * (double)g.Np / 5.0e12 + 6e-6;
     int U = (int)std::ceil(0.5e-3 / est_iter_s);
     U = std::max(2, std::min(U, 32));
     if (!graph_exec || graph_U != U || graph_kind != ifprec) {
@@ -1772,3 +1782,399 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
 }
 
 }  // namespace pot3d
+
+// ============================================================================
+// Batched PCG: many independent cases (uneven grids, own Br maps, own outer
+// radius) advanced together.  One launch of each tiled kernel covers the
+// tiles of every unfinished instance: the flat grid is the concatenation of
+// the instances' tile grids and each block finds its instance in a table of
+// block offsets; instances carry their own tensor maps, vectors, scalars and
+// reduction slots, so every instance converges on its own (blocks of a
+// finished instance return at once).  All iterations run from CUDA graphs.
+// ============================================================================
+namespace pot3d {
+
+struct alignas(64) BatchInst {
+  StencilMaps maps[2];  // parity 0: p_old = d_p; parity 1: p_old = d_p2
+  StencilArgs sa[2];
+  UpdateArgs ua[2];
+  Geo g;
+  DevMesh m;
+  unsigned off_s, off_u;
+};
+
+__device__ __forceinline__ int batch_find(const BatchInst *__restrict__ in, int n, unsigned blk, bool upd) {
+  int i = 0;
+  for (int q = 1; q < n; q++)
+    if ((upd ? in[q].off_u : in[q].off_s) <= blk) i = q;
+  return i;
+}
+
+__global__ void __launch_bounds__(NTHR, 2) k_stencil_batch(const BatchInst *__restrict__ in, int n, int par) {
+  const int i = batch_find(in, n, blockIdx.x, false);
+  const BatchInst &I = in[i];
+  const Geo g = I.g;
+  const DevMesh m = I.m;
+  const StencilArgs a = I.sa[par];
+  const unsigned local = blockIdx.x - I.off_s;
+  if (threadIdx.x == 0) {  // the thread that issues the TMA loads
+    tma_acquire_desc(&I.maps[par].m64[0]);
+    tma_acquire_desc(&I.maps[par].m64[1]);
+    tma_acquire_desc(&I.maps[par].m32[0]);
+  }
+  stencil_body<MODE_PCG>(I.maps[par], g, m, a, local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
+}
+
+__global__ void __launch_bounds__(NTHR) k_update_batch(const BatchInst *__restrict__ in, int n, int par) {
+  const int i = batch_find(in, n, blockIdx.x, true);
+  const BatchInst &I = in[i];
+  const Geo &g = I.g;
+  const unsigned local = blockIdx.x - I.off_u;
+  update_body<UPD_ITER, false>(g, I.m, I.ua[par], local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
+}
+
+struct Batch {
+  std::vector<Solver *> inst;
+  std::vector<int> act;        // cases in the current table (running ones)
+  BatchInst *d_tab = nullptr;  // capacity inst.size()
+  std::vector<BatchInst> h_tab;
+  unsigned nblk_s = 0, nblk_u = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  SolveState *pin = nullptr;  // pinned copies of the cases' states
+  cudaGraphExec_t graph = nullptr;
+  std::vector<int> graph_act;  // the table the graph was captured for
+  int U = 8;
+  int tk = 0;  // stencil planes per block (0 = per-case default)
+  ~Batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (d_tab) cudaFree(d_tab);
+    if (pin) cudaFreeHost(pin);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    for (Solver *s : inst) delete s;
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+// Apply the planes per block to every case (0 keeps each case's default).
+static void batch_set_tk(Batch &B, int tk) {
+  for (Solver *sp : B.inst) {
+    Solver &s = *sp;
+    if (tk > 0) {
+      s.g.tk = std::min(tk, std::min(s.g.npm2, MAX_TK));
+      s.g.nkc = (s.g.npm2 + s.g.tk - 1) / s.g.tk;
+    } else {
+      s.g.tk = s.tk_default;
+      s.g.nkc = s.nkc_default;
+    }
+  }
+  B.tk = tk;
+}
+
+// Build and upload the instance table of the cases in B.act.
+static int batch_table(Batch &B) {
+  B.h_tab.assign(B.act.size(), BatchInst{});
+  unsigned os = 0, ou = 0;
+  for (size_t t = 0; t < B.act.size(); t++) {
+    Solver &s = *B.inst[B.act[t]];
+    BatchInst &I = B.h_tab[t];
+    I.g = s.g;
+    I.m = s.m;
+    for (int par = 0; par < 2; par++) {
+      double *pold = par == 0 ? s.d_p : s.d_p2, *pnew = par == 0 ? s.d_p2 : s.d_p;
+      StencilArgs &sa = I.sa[par];
+      sa = StencilArgs{};
+      sa.p_old = pold;
+      sa.p_new = pnew;
+      sa.r = s.d_r;
+      sa.ai = s.d_ai;
+      sa.q = s.d_q;
+      sa.s1z_part = s.d_s1z;
+      sa.s1p = s.d_s1p;
+      sa.st = s.d_state;
+      sa.partials = s.d_partials;
+      UpdateArgs &ua = I.ua[par];
+      ua = UpdateArgs{};
+      ua.x = s.d_x;
+      ua.p = pnew;
+      ua.r = s.d_r;
+      ua.q = s.d_q;
+      ua.ai = s.d_ai;
+      ua.s1z_part = s.d_s1z;
+      ua.st = s.d_state;
+      ua.partials = s.d_partials;
+      int st;
+      if ((st = s.tensor_map(pold, true, &I.maps[par].m64[0])) || (st = s.tensor_map(s.d_r, true, &I.maps[par].m64[1])) ||
+          (st = s.tensor_map(s.d_ai, false, &I.maps[par].m32[0])))
+        return st;
+      I.maps[par].m32[1] = I.maps[par].m32[2] = I.maps[par].m32[0];
+    }
+    I.off_s = os;
+    I.off_u = ou;
+    os += (unsigned)s.g.nit * s.g.njt * s.g.nkc;
+    ou += (unsigned)s.g.nit * s.g.njt * s.g.nkc_u;
+  }
+  B.nblk_s = os;
+  B.nblk_u = ou;
+  if (B.act.empty()) return POT3D_OK;
+  return pot3d_cuda_status(
+      cudaMemcpyAsync(B.d_tab, B.h_tab.data(), sizeof(BatchInst) * B.act.size(), cudaMemcpyHostToDevice, B.stream),
+      "cudaMemcpy(batch table)");
+}
+
+static int batch_init(Batch &B, int ncgmax, double epscg) {
+  for (Solver *sp : B.inst) {
+    Solver &s = *sp;
+    SolveState s0{};
+    s0.epscg = epscg;
+    s0.ncgmax = ncgmax;
+    s0.hist = nullptr;
+    CK(cudaMemcpyAsync(s.d_state, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, B.stream));
+    CK(cudaMemsetAsync(s.d_x, 0, sizeof(double) * s.g.Np, B.stream));
+    CK(cudaMemsetAsync(s.d_p, 0, sizeof(double) * s.g.Np, B.stream));
+    CK(cudaMemsetAsync(s.d_s1p, 0, sizeof(double) * 2 * s.g.NRP, B.stream));
+    CK(cudaMemcpyAsync(s.d_r, s.d_b, sizeof(double) * s.g.Np, cudaMemcpyDeviceToDevice, B.stream));
+    dim3 gridu(s.g.nit, s.g.njt, s.g.nkc_u);
+    UpdateArgs ua{};
+    ua.x = s.d_x;
+    ua.p = s.d_p;
+    ua.r = s.d_r;
+    ua.q = s.d_q;
+    ua.ai = s.d_ai;
+    ua.s1z_part = s.d_s1z;
+    ua.st = s.d_state;
+    ua.partials = s.d_partials;
+    k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+    k_update<UPD_INIT, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+  }
+  return pot3d_cuda_status(cudaGetLastError(), "batch_init");
+}
+
+static void batch_iteration(Batch &B, int par) {
+  const int n = (int)B.act.size();
+  k_stencil_batch<<<B.nblk_s, NTHR, StageLayout<MODE_PCG>::smem, B.stream>>>(B.d_tab, n, par);
+  k_update_batch<<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+}
+
+// Capture 2U batched iterations of the current table into B.graph.
+static int batch_capture(Batch &B) {
+  if (B.graph) cudaGraphExecDestroy(B.graph);
+  B.graph = nullptr;
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
+  for (int u = 0; u < 2 * B.U; u++) batch_iteration(B, u & 1);  // even: parity returns to 0
+  CK(cudaStreamEndCapture(B.stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&B.graph, graph, 0);
+  cudaGraphDestroy(graph);
+  CK(e);
+  B.graph_act = B.act;
+  return POT3D_OK;
+}
+
+// Time a few iterations of the batch with the current table (all instances
+// running); used by the autotuner.
+static int batch_time(Batch &B, int iters, float *ms) {
+  int st;
+  if ((st = batch_init(B, 0x7fffffff, 0.0))) return st;
+  batch_iteration(B, 0);
+  batch_iteration(B, 1);
+  CK(cudaEventRecord(B.ev0, B.stream));
+  for (int it = 0; it < iters; it++) batch_iteration(B, it & 1);
+  CK(cudaEventRecord(B.ev1, B.stream));
+  CK(cudaEventSynchronize(B.ev1));
+  cudaEventElapsedTime(ms, B.ev0, B.ev1);
+  return pot3d_cuda_status(cudaGetLastError(), "batch_time");
+}
+
+static int batch_poll(Batch &B) {
+  for (int q : B.act)
+    CK(cudaMemcpyAsync(B.pin + q, B.inst[q]->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, B.stream));
+  return pot3d_cuda_status(cudaStreamSynchronize(B.stream), "batch poll");
+}
+
+}  // namespace pot3d
+
+struct pot3d_gpu_batch {
+  pot3d::Batch b;
+};
+
+extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                                      const double *pm_r1s, int tk, pot3d_gpu_batch **out) {
+  using namespace pot3d;
+  if (n < 1 || !meshes || !br0s || !pm_r1s || !out) {
+    pot3d_set_error("pot3d_gpu_batch_create: invalid arguments");
+    return POT3D_ERR_ARG;
+  }
+  if (tk != 0 && (tk < 8 || tk > MAX_TK)) {
+    pot3d_set_error("pot3d_gpu_batch_create: planes per block must be 0 or in [8, 512]");
+    return POT3D_ERR_ARG;
+  }
+  *out = nullptr;
+  pot3d_gpu_batch *h = new pot3d_gpu_batch();
+  Batch &B = h->b;
+  int st = pot3d_cuda_status(cudaStreamCreate(&B.stream), "cudaStreamCreate");
+  if (!st) st = pot3d_cuda_status(cudaEventCreate(&B.ev0), "cudaEventCreate");
+  if (!st) st = pot3d_cuda_status(cudaEventCreate(&B.ev1), "cudaEventCreate");
+  if (!st) st = pot3d_cuda_status(cudaMallocHost(&B.pin, sizeof(SolveState) * n), "cudaMallocHost");
+  if (!st) st = pot3d_cuda_status(cudaMalloc(&B.d_tab, sizeof(BatchInst) * n), "cudaMalloc(batch table)");
+  for (int q = 0; q < n && !st; q++) {
+    Solver *s = new Solver();
+    B.inst.push_back(s);
+    st = s->setup(&meshes[q], br0s[q], nullptr, pm_r1s[q], 1, POT3D_FP64);
+    if (!st) {
+      s->tk_default = s->g.tk;
+      s->nkc_default = s->g.nkc;
+      // reduction slots of the stencil for any planes per block >= 8
+      const size_t need = (size_t)s->g.nit * s->g.njt * ((s->g.npm2 + 7) / 8);
+      if (need > std::max<size_t>(s->nblk_tiled, 148 * 16 * 3))
+        st = s->alloc((void **)&s->d_partials, sizeof(double) * need);
+    }
+  }
+  // the cases' setup ran on their own streams
+  if (!st) st = pot3d_cuda_status(cudaDeviceSynchronize(), "batch setup");
+  if (!st)
+    st = pot3d_cuda_status(cudaFuncSetAttribute(k_stencil_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                StageLayout<MODE_PCG>::smem),
+                           "cudaFuncSetAttribute(k_stencil_batch)");
+  if (st) {
+    delete h;
+    return st;
+  }
+  batch_set_tk(B, tk);
+  *out = h;
+  return POT3D_OK;
+}
+
+// Autotuner: times `iters` batched iterations of all cases for each candidate
+// planes per block; applies and returns the fastest.
+extern "C" int pot3d_gpu_batch_tune(pot3d_gpu_batch *h, const int *candidates, int ncand, int iters, int *best_tk,
+                                    float *ms_out) {
+  using namespace pot3d;
+  if (!h || !candidates || ncand < 1 || iters < 1) {
+    pot3d_set_error("pot3d_gpu_batch_tune: invalid arguments");
+    return POT3D_ERR_ARG;
+  }
+  Batch &B = h->b;
+  for (int c = 0; c < ncand; c++)
+    if (candidates[c] < 8 || candidates[c] > MAX_TK) {
+      pot3d_set_error("pot3d_gpu_batch_tune: planes per block must be in [8, 512]");
+      return POT3D_ERR_ARG;
+    }
+  float best = 1e30f;
+  int bt = candidates[0], st;
+  B.act.resize(B.inst.size());
+  for (size_t q = 0; q < B.inst.size(); q++) B.act[q] = (int)q;
+  for (int c = 0; c < ncand; c++) {
+    batch_set_tk(B, candidates[c]);
+    if ((st = batch_table(B))) return st;
+    float ms = 0.f;
+    if ((st = batch_time(B, iters, &ms))) return st;
+    if (ms_out) ms_out[c] = ms;
+    if (ms < best) {
+      best = ms;
+      bt = candidates[c];
+    }
+  }
+  batch_set_tk(B, bt);
+  B.graph_act.clear();  // the graph (if any) belongs to another tiling
+  if (best_tk) *best_tk = bt;
+  return POT3D_OK;
+}
+
+extern "C" int pot3d_gpu_batch_solve(pot3d_gpu_batch *h, int ncgmax, double epscg, int *ierr,
+                                     pot3d_solve_info_t *info, double *seconds) {
+  using namespace pot3d;
+  if (!h) {
+    pot3d_set_error("null batch");
+    return POT3D_ERR_ARG;
+  }
+  Batch &B = h->b;
+  const int n = (int)B.inst.size();
+  int st;
+  CK(cudaEventRecord(B.ev0, B.stream));
+  if ((st = batch_init(B, ncgmax, epscg))) return st;
+  B.act.resize(n);
+  for (int q = 0; q < n; q++) B.act[q] = q;
+  if ((st = batch_poll(B))) return st;
+  long long launches = 2LL * n;
+  // Zero right-hand side -> zero solution (src/pot3d.F90:4302-4311).
+  for (int q = 0; q < n; q++)
+    if (B.pin[q].bdotb == 0.0) {
+      B.pin[q].status = ST_CONVERGED;
+      B.pin[q].ncg = 0;
+      B.pin[q].epsn = 0.0;
+      CK(cudaMemcpyAsync(B.inst[q]->d_state, &B.pin[q], sizeof(SolveState), cudaMemcpyHostToDevice, B.stream));
+    }
+  // Loop: run 2U iterations of the running cases from a graph, read their
+  // states, drop the finished ones from the table (so later launches cover
+  // only running cases' tiles) and re-capture when the set changed.
+  int last_total = -1, stalls = 0;
+  for (;;) {
+    std::vector<int> run;
+    int total = 0;
+    for (int q : B.act) {
+      if (B.pin[q].status == ST_RUNNING) run.push_back(q);
+      total += B.pin[q].ncg;
+    }
+    if (run.empty()) break;
+    if (total <= last_total) {
+      if (++stalls >= 3) {
+        pot3d_set_error("batched PCG state stopped advancing on the device");
+        return POT3D_ERR_TIMEOUT;
+      }
+    } else {
+      stalls = 0;
+    }
+    last_total = total;
+    if (run != B.act || !B.graph || B.graph_act != run) {
+      B.act = run;
+      if ((st = batch_table(B)) || (st = batch_capture(B))) return st;
+    }
+    CK(cudaGraphLaunch(B.graph, B.stream));
+    launches += 4LL * B.U;
+    if ((st = batch_poll(B))) return st;
+  }
+  CK(cudaEventRecord(B.ev1, B.stream));
+  CK(cudaEventSynchronize(B.ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, B.ev0, B.ev1);
+  for (int q = 0; q < n; q++) {
+    if (ierr) ierr[q] = B.pin[q].status == ST_CONVERGED ? 0 : 1;
+    if (info) {
+      info[q] = pot3d_solve_info_t{};
+      info[q].ncg = B.pin[q].ncg;
+      info[q].epsn = B.pin[q].epsn;
+      info[q].seconds = ms * 1e-3;
+      info[q].kernel_launches = launches;
+    }
+  }
+  for (int q = 0; q < n; q++)
+    if (B.pin[q].status == ST_BREAKDOWN || B.pin[q].status == ST_TIMEOUT) {
+      const bool bd = B.pin[q].status == ST_BREAKDOWN;
+      pot3d_set_error(std::string(bd ? "batched PCG breakdown in case " : "TMA wait timed out in case ") +
+                      std::to_string(q));
+      return bd ? POT3D_ERR_BREAKDOWN : POT3D_ERR_TIMEOUT;
+    }
+  if (seconds) *seconds = ms * 1e-3;
+  return POT3D_OK;
+}
+
+extern "C" int pot3d_gpu_batch_solution(pot3d_gpu_batch *h, int i, double *x) {
+  using namespace pot3d;
+  if (!h || i < 0 || i >= (int)h->b.inst.size() || !x) {
+    pot3d_set_error("pot3d_gpu_batch_solution: invalid arguments");
+    return POT3D_ERR_ARG;
+  }
+  Solver &s = *h->b.inst[i];
+  int st;
+  if ((st = s.unpack(s.d_x, reinterpret_cast<double *>(s.d_tmp)))) return st;
+  CK(cudaStreamSynchronize(s.stream));
+  CK(cudaMemcpy(x, s.d_tmp, sizeof(double) * s.g.N, cudaMemcpyDeviceToHost));
+  return POT3D_OK;
+}
+
+extern "C" int pot3d_gpu_batch_destroy(pot3d_gpu_batch *h) {
+  delete h;
+  return POT3D_OK;
+}

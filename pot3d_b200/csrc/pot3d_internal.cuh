@@ -85,14 +85,13 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return s;
 }
 
-// Last-block pattern: every block stores its partial, the block that
-// arrives last sums all partials in index order (deterministic for a fixed
-// grid) and returns true in all its threads with the total in *total.
+// Last-block pattern: every block stores its partial at slot b, the block
+// that arrives last sums all partials in index order (deterministic for a
+// fixed grid) and returns true in all its threads with the total in *total.
 template <int NT>
-__device__ bool last_block_sum(double part, double *partials, unsigned int *counter,
-                               unsigned int nblocks, double *total, double *sh) {
+__device__ bool last_block_sum_at(double part, double *partials, unsigned int *counter, unsigned int nblocks,
+                                  unsigned int b, double *total, double *sh) {
   __shared__ bool is_last;
-  const unsigned int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (threadIdx.x == 0) {
     partials[b] = part;
     __threadfence();
@@ -111,9 +110,23 @@ __device__ bool last_block_sum(double part, double *partials, unsigned int *coun
   }
   return true;
 }
+template <int NT>
+__device__ bool last_block_sum(double part, double *partials, unsigned int *counter, unsigned int nblocks,
+                               double *total, double *sh) {
+  const unsigned int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  return last_block_sum_at<NT>(part, partials, counter, nblocks, b, total, sh);
+}
 
 }  // namespace pot3d
 
 // Error reporting shared by the C-ABI entry points.
 void pot3d_set_error(const std::string &msg);
+
+// Return the library status of a failing CUDA runtime call.
+#define CK(call)                                                  \
+  do {                                                            \
+    int _st = pot3d_cuda_status((call), #call);                   \
+    if (_st != POT3D_OK) return _st;                              \
+  } while (0)
+
 int pot3d_cuda_status(cudaError_t e, const char *where);

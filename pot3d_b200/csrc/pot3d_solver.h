@@ -27,6 +27,7 @@ struct Solver {
   SolveState *h_state = nullptr;
   double *d_partials = nullptr;
   size_t nblk_tiled = 0;
+  int tk_default = 0, nkc_default = 0;  // stencil k-chunking chosen at setup
   double *d_s1z = nullptr, *d_s1p = nullptr, *d_s1 = nullptr;
   double *d_scalar = nullptr, *d_sums = nullptr, *d_hist = nullptr;
   int hist_cap = 0;
@@ -89,6 +90,8 @@ float *dilu_z32(Solver *s);   // FP32 output z = (LU)^-1 r32
 // Forward + backward sweeps r32 -> z32 on s->stream; with check_status the
 // kernels return at once when the PCG state is no longer running.
 int dilu_sweeps(Solver *s, bool check_status);
+int dilu_reset(Solver *s);
+int dilu_status(Solver *s);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
 int dilu_diag(Solver *s, float *d_host, float *dinv_host);
 int dilu_sweep_launches(Solver *s);
 

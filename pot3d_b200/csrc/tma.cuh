@@ -54,4 +54,11 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// A tensor map that reached global memory by a host copy must be acquired by
+// the tensormap proxy before the first TMA use from that address.
+__device__ __forceinline__ void tma_acquire_desc(const CUtensorMap *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
 }  // namespace pot3d

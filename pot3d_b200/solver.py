@@ -153,3 +153,76 @@ def potfld(mesh: Mesh, br0, option="ss", ifprec=1, precision="fp64", epscg=1e-9,
         return dict(x=x, r=r, rhs=b, ierr=ierr, ncg=info.ncg, epsn=info.epsn, true_resid=info.true_resid,
                     seconds=info.seconds, n_refine=info.n_refine, launches=info.kernel_launches, phi=phi, energy=w,
                     history=s.history())
+
+
+class BatchSolver:
+    """Many independent PCG solves (own grid, Br map and outer radius each)
+    advanced together by the batched kernels: every launch covers the tiles of
+    all unfinished cases, each case stops at its own ernorm criterion.  FP64
+    PCG with the diagonal preconditioner (ifprec=1), zero initial guess.
+    """
+
+    def __init__(self, meshes, br0s, pm_r1s, tk: int = 0):
+        if not (len(meshes) == len(br0s) == len(pm_r1s)) or not meshes:
+            raise ValueError("meshes, br0s and pm_r1s must be non-empty and of equal length")
+        n = len(meshes)
+        self.meshes = list(meshes)
+        self._br = [np.asfortranarray(b, dtype=np.float64) for b in br0s]
+        for m, b in zip(self.meshes, self._br):
+            if b.shape != (m.nt, m.np):
+                raise ValueError("br0 must have shape (nt, np) of its mesh")
+        self._mcs = (_lib.MeshC * n)(*[m.cstruct() for m in self.meshes])
+        self._keep = [m for m in self.meshes]  # keep mesh arrays alive
+        self._brp = (C.POINTER(C.c_double) * n)(*[dptr(b) for b in self._br])
+        self._r1 = np.ascontiguousarray(pm_r1s, dtype=np.float64)
+        h = C.c_void_p()
+        check(_lib.lib().pot3d_gpu_batch_create(n, self._mcs, self._brp, dptr(self._r1), tk, C.byref(h)))
+        self._h = h
+        self.n = n
+        self.tk = tk
+        self.infos = None
+        self.seconds = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().pot3d_gpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def tune(self, candidates=(8, 16, 24, 32, 48, 64), iters: int = 6):
+        """Pick the stencil's planes per block by timing; returns
+        (best, {candidate: ms})."""
+        c = (C.c_int * len(candidates))(*candidates)
+        ms = (C.c_float * len(candidates))()
+        best = C.c_int(0)
+        check(_lib.lib().pot3d_gpu_batch_tune(self._h, c, len(candidates), iters, C.byref(best), ms))
+        self.tk = best.value
+        return best.value, {int(k): float(v) for k, v in zip(candidates, ms)}
+
+    def solve(self, epscg: float = 1e-9, ncgmax: int = 10_000_000):
+        """Solve every case; returns the list of ierr (0 = converged)."""
+        ierr = (C.c_int * self.n)()
+        infos = (SolveInfo * self.n)()
+        sec = C.c_double(0.0)
+        check(_lib.lib().pot3d_gpu_batch_solve(self._h, ncgmax, epscg, ierr, infos, C.byref(sec)))
+        self.infos = list(infos)
+        self.seconds = sec.value
+        return list(ierr)
+
+    def solution(self, i: int) -> np.ndarray:
+        """Interior solution of case i, packed layout (length N_i)."""
+        m = self.meshes[i]
+        x = np.zeros((m.nr - 2) * (m.nt - 2) * (m.np - 2))
+        check(_lib.lib().pot3d_gpu_batch_solution(self._h, i, dptr(x)))
+        return x

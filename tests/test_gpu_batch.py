@@ -1,0 +1,86 @@
+"""Batched PCG over uneven grids against single-case solves.
+
+With the default planes per block every case runs the same tiles and the same
+reduction order as its single-case solve, so iteration counts and solutions
+must agree bit for bit; a tuned planes-per-block changes only the summation
+order of the reductions (iterations within 1, solutions to 1e-9 relative).
+"""
+import numpy as np
+import pytest
+
+from pot3d_b200 import host
+from pot3d_b200.host import PM_R1
+from pot3d_b200.solver import BatchSolver, Pot3dSolver
+
+pytestmark = pytest.mark.gpu
+
+DIMS = [(33, 41, 65, 2.0), (25, 31, 48, 2.7), (41, 37, 73, 3.0), (20, 13, 11, 2.3)]
+
+
+def _cases():
+    out = []
+    for q, (nr, nt, np_, r1) in enumerate(DIMS):
+        mesh = host.make_mesh(nr, nt, np_, r1=r1)
+        tn, pn, fi = host.synthetic_br(100 + q, 15, 4, nt, np_)
+        out.append((mesh, host.br0_from_map(mesh, tn, pn, fi)))
+    return out
+
+
+def _single(mesh, br0, epscg):
+    with Pot3dSolver(mesh, br0) as s:
+        x = np.zeros(s.N)
+        r = s.rhs()
+        ierr = s.cgsolve(x, r, epscg=epscg)
+        return ierr, s.last_info.ncg, x
+
+
+def test_batch_matches_single_solves_bitwise(cuda):
+    cases = _cases()
+    with BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * len(cases)) as b:
+        ierr = b.solve(epscg=1e-10)
+        assert ierr == [0] * len(cases)
+        ncgs = [i.ncg for i in b.infos]
+        assert len(set(ncgs)) > 1  # the cases stop at different iterations
+        for q, (mesh, br0) in enumerate(cases):
+            e1, n1, x1 = _single(mesh, br0, 1e-10)
+            assert e1 == 0 and n1 == ncgs[q]
+            assert np.array_equal(b.solution(q), x1)
+        # a second solve on the same batch (graph reused) repeats the first
+        x0 = b.solution(0)
+        assert b.solve(epscg=1e-10) == [0] * len(cases)
+        assert [i.ncg for i in b.infos] == ncgs
+        assert np.array_equal(b.solution(0), x0)
+
+
+def test_batch_tuned_planes_per_block(cuda):
+    cases = _cases()
+    with BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * len(cases)) as b:
+        best, times = b.tune(candidates=(8, 16, 32), iters=4)
+        assert best in (8, 16, 32) and all(t > 0 for t in times.values())
+        assert b.solve(epscg=1e-10) == [0] * len(cases)
+        for q, (mesh, br0) in enumerate(cases):
+            e1, n1, x1 = _single(mesh, br0, 1e-10)
+            assert abs(b.infos[q].ncg - n1) <= 1
+            x = b.solution(q)
+            assert np.linalg.norm(x - x1) <= 1e-9 * np.linalg.norm(x1)
+
+
+def test_batch_zero_rhs_case(cuda):
+    cases = _cases()[:2]
+    cases[1] = (cases[1][0], np.zeros_like(cases[1][1]))
+    with BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * 2) as b:
+        assert b.solve(epscg=1e-10) == [0, 0]
+        assert b.infos[1].ncg == 0
+        assert not b.solution(1).any()
+        e1, n1, x1 = _single(*cases[0], 1e-10)
+        assert b.infos[0].ncg == n1 and np.array_equal(b.solution(0), x1)
+
+
+def test_batch_rejects_bad_arguments(cuda):
+    from pot3d_b200._lib import Pot3dError
+    mesh, br0 = _cases()[0]
+    with pytest.raises(Pot3dError):
+        BatchSolver([mesh], [br0], [1.0], tk=3)
+    with BatchSolver([mesh], [br0], [1.0]) as b:
+        with pytest.raises(Pot3dError):
+            b.tune(candidates=(4,))

@@ -138,3 +138,13 @@ def test_library_exports_every_declared_symbol():
     assert {"load_external_lu_solver", "external_lu_solver", "pot3d_gpu_cgsolve"} <= syms
     missing = [s for s in sorted(syms) if not hasattr(L, s)]
     assert not missing, missing
+
+
+def test_batch_specs_cover_the_uneven_grid_law():
+    from pot3d_b200.batch import NP, NR, NT, batch_specs
+    s = batch_specs(48, 0)
+    assert len(s) == 48 and s == batch_specs(48, 0)
+    assert {x[0] for x in s} <= set(NR) and {x[1] for x in s} <= set(NT) and {x[2] for x in s} <= set(NP)
+    assert len({x[:3] for x in s}) > 4  # uneven
+    assert all(2.0 <= x[3] <= 3.0 for x in s)
+    assert len({x[4] for x in s}) == 48  # own Br seed per case
