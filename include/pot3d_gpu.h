@@ -169,6 +169,11 @@ int pot3d_gpu_precond_diag(pot3d_gpu_solver *s, float *d, float *dinv);
  * algorithmic DRAM bytes per launch (stencil: r, p read, p, Ap written;
  * update: x, p, r, Ap read, x, r written; 8 B each per unknown). */
 int pot3d_gpu_time_kernels(pot3d_gpu_solver *s, int reps, double ms[2], double bytes[2]);
+/* Average device milliseconds of the ILU(0) forward (ms[0]) and backward
+ * (ms[1]) wavefront sweeps over `reps` applications (ifprec = 2 only).
+ * No counterpart in the reference (its timers cover whole preconditioner
+ * calls, src/pot3d.F90 timing.out "PC"). */
+int pot3d_gpu_time_sweeps(pot3d_gpu_solver *s, int reps, double ms[2]);
 
 /* Magnetic energies like pot3d_gpu_energy, for callers that cannot allocate
  * device memory (their memory is owned by another allocator, or they run

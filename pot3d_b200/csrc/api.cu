@@ -224,6 +224,16 @@ extern "C" int pot3d_gpu_time_kernels(pot3d_gpu_solver *h, int reps, double ms[2
   return h->s.time_kernels(reps, ms, bytes);
 }
 
+extern "C" int pot3d_gpu_time_sweeps(pot3d_gpu_solver *h, int reps, double ms[2]) {
+  int st;
+  if ((st = check_solver(h))) return st;
+  if (reps <= 0 || h->s.ifprec != 2 || !ms) {
+    pot3d_set_error("time_sweeps: reps must be positive and ifprec 2");
+    return POT3D_ERR_ARG;
+  }
+  return pot3d::dilu_time(&h->s, reps, ms);
+}
+
 extern "C" int pot3d_gpu_set_br0(pot3d_gpu_solver *h, const double *br0) {
   int st;
   if ((st = check_solver(h))) return st;

@@ -110,27 +110,41 @@ __global__ void k_dilu_factor(LevelArgs a) {
 }
 
 // ============================================================================
-// Wavefront sweeps.  One persistent kernel per triangular solve.  The (j, k)
-// lines of the interior are cut into tiles of 4 x 8 lines; one warp owns a
-// tile for the whole radial extent, lane (jl, kl) = (lane & 3, lane >> 2)
-// owning one line.  Lanes are skewed by s = jl + kl steps (mirrored in the
-// backward sweep), so at its step t a lane handles point e = t - s and the
-// lower neighbours it needs, (e, j-1, k) and (e, j, k-1), were produced by
-// lanes L-1 and L-4 one step earlier: a warp shuffle.  Across tile faces,
-// and through the periodic seam, values travel as 64-bit words holding the
-// FP32 value and a sweep tag, written once and polled by the consumer until
-// the tag matches (bounded spin; a timeout marks the solve state).  Warps
-// take tiles in the order of the tickets of a global counter, sorted so
-// every tile's producers hold smaller tickets: a warp only ever waits on a
-// tile already owned by a running warp, so the kernel needs no co-residency.
-// The last warp to finish resets the counter and advances the sweep tag.
-// Every value is computed with the level kernels' operations in the same
-// order (the reference's lusol), so the result is bit-identical to them.
+// Wavefront sweeps.  One persistent kernel per triangular solve.
+//
+// Each thread owns one radial-latitude line (e, j) and walks it along phi
+// (k), so the periodic seam coupling between the first and the last phi
+// plane stays in the thread's registers.  A block owns a tile of 16 x 16
+// lines; thread (el, jl) is skewed by s = el + jl steps (mirrored in the
+// backward sweep), so at step t it handles plane k = t - s and its
+// neighbours (e-1, j, k) and (e, j-1, k) were produced by the threads
+// (el-1, jl) and (el, jl-1) one step earlier: the block runs in lockstep,
+// one barrier per step, and exchanges them through shared memory.
+//
+// Across tile faces values travel as 64-bit words holding the FP32 value
+// and a sweep tag.  A word is indexed by the step at which its consumer
+// needs it, so the words of one face for 8 consecutive steps are one
+// contiguous block; the whole block fetches the next 8 steps' words (and,
+// forward, the neighbour pivots) one chunk ahead, checks their tags when
+// the chunk starts and polls again (bounded) only for words not yet
+// written.  Tiles are taken in the order of the tickets of a global
+// counter, sorted so that every tile's producers (e-1 and j-1 faces)
+// hold smaller tickets: a block only ever waits for a tile already owned
+// by a running block, and the kernel needs no co-residency.  The last
+// block to finish resets the counter and advances the tag.
+//
+// Every value is computed with the operations, and in the order, of the
+// reference's lusol (src/pot3d.F90:5227-5302), so the sweeps are
+// bit-identical to it.
 // ============================================================================
-constexpr int WJ = 4, WK = 8;           // lines per tile in j and k
-constexpr int WAVE_THREADS = 128;
-constexpr int WAVE_PF = 8;              // prefetch distance (steps) of the point loads
+constexpr int WE = 16, WJT = 16;        // lines per tile in e and j
+constexpr int WAVE_THREADS = WE * WJT;  // one thread per line
+constexpr int WCH = 8;                  // steps per exchange chunk
+constexpr int WPF = 4;                  // prefetch distance of the point loads (steps)
+constexpr int WSK = (WE - 1) + (WJT - 1);
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
+static_assert(2 * WCH * 16 == WAVE_THREADS, "one exchange word per thread and chunk");
+static_assert(WCH % WPF == 0, "chunk is a whole number of prefetch rounds");
 
 struct WaveCtl {
   unsigned ticket, done, epoch;
@@ -143,284 +157,292 @@ struct WaveArgs {
   const float *in;    // forward: r32 ; backward: y32
   float *out;         // forward: y32 ; backward: z32
   const float *d;     // forward: factor diagonal d ; backward: dinv
-  unsigned long long *xj, *xk, *xs;  // tile-face and seam exchange words
-  const int2 *order;  // ticket -> tile (tj, tk) in forward order
+  const float *dfac;  // factor diagonal d (forward neighbour pivots)
+  unsigned long long *xe, *xj;  // e-face and j-face exchange words
+  const int2 *order;  // ticket -> tile (te, tj) in forward order
   WaveCtl *ctl;
   SolveState *st;
   int check;          // skip when the solve state is no longer running
-  int ntj, ntk, ntiles;
+  int nte, ntj, ntiles, ndiag;
 };
 
 __device__ __forceinline__ void wave_publish(unsigned long long *p, unsigned epoch, float v) {
   const unsigned long long w = ((unsigned long long)epoch << 32) | __float_as_uint(v);
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
 }
-__device__ __forceinline__ bool wave_take(const unsigned long long *p, unsigned epoch, float *v) {
+__device__ __forceinline__ unsigned long long wave_load(const unsigned long long *p) {
   unsigned long long w;
-  for (unsigned it = 0;; it++) {
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
-    if ((unsigned)(w >> 32) == epoch) break;
-    if (it >= WAVE_SPIN_LIMIT) return false;
-    if (it >= 16) __nanosleep(64);
-  }
-  *v = __uint_as_float((unsigned)w);
-  return true;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+  return w;
 }
 
-// Forward solve of one tile: y = r - sum_{lower} (a/d) y, lusol's row order
-// [seam, k-1, j-1, i-1].  Returns false on an exchange timeout.
-__device__ __forceinline__ bool wave_tile_forward(const WaveArgs &a, const double *sh, unsigned epoch, int tj,
-                                                  int tk, int lane) {
+struct WaveSmem {
+  float y[2][WJT][WE + 1];           // step parity, line values
+  float dv[2][WJT][WE + 1];          // forward: the lines' pivots d at their current point
+  float ring[2][2][WCH][16];         // chunk parity, face (0: e, 1: j), step in chunk, line
+  float dring[2][2][WCH][16];        // forward: pivots of the neighbours across the faces
+  int2 tile;
+  int abort;
+};
+
+// Exchange slot (face, step s of chunk, line) of thread T.
+__device__ __forceinline__ void wave_slot(int T, int *f, int *s, int *line) {
+  *f = T >> 7;
+  *s = (T >> 4) & (WCH - 1);
+  *line = T & 15;
+}
+
+template <bool FWD>
+__device__ __forceinline__ bool wave_tile(const WaveArgs &a, WaveSmem &S, const double *kdph, const double *kdpi,
+                                          unsigned epoch, int te, int tj) {
   const Geo &g = a.g;
   const DevMesh &m = a.m;
-  const int jl = lane & 3, kl = lane >> 2;
-  const int jj = tj * WJ + jl, kk = tk * WK + kl;
-  const bool valid = jj < g.ntm2 && kk < g.npm2;
-  const int sk = jl + kl;
-  const int nr2 = g.nrm2;
-  const double *sh_drh = sh, *sh_r2 = sh + nr2, *sh_dri = sh + 2 * nr2;
-  double dth_j = 0, sthi_j = 0, dpi_km1 = 0, dpi_k = 0, dph_k = 0, st_jm1 = 0, dti_jm1 = 0, v = 0;
-  if (valid) {
-    const int j = jj + 2, k = kk + 2;
-    dth_j = m.dth[j];
-    sthi_j = m.sth_i[j];
-    dpi_km1 = m.dp_i[k - 1];
-    dpi_k = m.dp_i[k];
-    dph_k = m.dph[k];
-    st_jm1 = m.st[j - 1];
-    dti_jm1 = m.dt_i[j - 1];
-    v = __dmul_rn(__dmul_rn(m.sth[j], dth_j), dph_k);
-  }
-  const long long base = valid ? ((long long)kk * g.ntm2 + jj) * g.NRP : 0;
+  const int T = threadIdx.x;
+  const int el = T & (WE - 1), jl = T / WE;
+  const int e = te * WE + el, jj = tj * WJT + jl;
+  const bool valid = e < g.nrm2 && jj < g.ntm2;
+  const int sk = FWD ? el + jl : (WE - 1 - el) + (WJT - 1 - jl);
+  const int npm2 = g.npm2;
   const long long plane = (long long)g.ntm2 * g.NRP;
-  const bool use_seam = valid && kk == g.npm2 - 1;
-  const bool pub_j = valid && jl == WJ - 1 && tj + 1 < a.ntj;
-  const bool pub_k = valid && kl == WK - 1 && tk + 1 < a.ntk;
-  const bool pub_s = valid && kk == 0;
-  const unsigned long long *cj = tj > 0 ? a.xj + ((size_t)(tk * a.ntj + tj - 1) * WK + kl) * nr2 : a.xj;
-  const unsigned long long *ck = tk > 0 ? a.xk + ((size_t)((tk - 1) * a.ntj + tj) * WJ + jl) * nr2 : a.xk;
-  unsigned long long *pj = a.xj + ((size_t)(tk * a.ntj + tj) * WK + kl) * nr2;
-  unsigned long long *pk = a.xk + ((size_t)(tk * a.ntj + tj) * WJ + jl) * nr2;
-  unsigned long long *xs = a.xs + (size_t)jj * nr2;
-  const float *pin = a.in + base, *pd = a.d + base;
-  float *pout = a.out + base;
-  float rbuf[WAVE_PF], dbuf[WAVE_PF];
-#pragma unroll
-  for (int u = 0; u < WAVE_PF; u++) {  // points e = u - sk of the first steps
-    const int e = u - sk;
-    const bool ld = valid && e >= 0 && e < nr2;
-    rbuf[u] = ld ? pin[e] : 0.f;
-    dbuf[u] = ld ? pd[e] : 0.f;
-  }
-  float yprev = 0.f, dprev = 0.f;
-  bool ok = true;
-  const int nsteps = nr2 + (WJ - 1) + (WK - 1);
-  for (int t0 = 0; t0 < nsteps; t0 += WAVE_PF) {
-#pragma unroll
-    for (int u = 0; u < WAVE_PF; u++) {
-      const int t = t0 + u;
-      const float yj_in = __shfl_up_sync(0xffffffffu, yprev, 1);
-      const float yk_in = __shfl_up_sync(0xffffffffu, yprev, WJ);
-      const float dj_in = __shfl_up_sync(0xffffffffu, dprev, 1);
-      const float dk_in = __shfl_up_sync(0xffffffffu, dprev, WJ);
-      const int e = t - sk;
-      const float r_e = rbuf[u], d_e = dbuf[u];
-      {  // prefetch the point WAVE_PF steps ahead into the freed slot
-        const int ef = e + WAVE_PF;
-        const bool ld = valid && ef >= 0 && ef < nr2;
-        rbuf[u] = ld ? pin[ef] : 0.f;
-        dbuf[u] = ld ? pd[ef] : 0.f;
-      }
-      if (t < nsteps && valid && e >= 0 && e < nr2) {
-        const double drh = sh_drh[e];
-        const double c17 = __dmul_rn(__dmul_rn(drh, dth_j), sthi_j);
-        float y = r_e;
-        if (use_seam) {
-          const float aik = __double2float_rn(-__dmul_rn(c17, dpi_k));
-          float ys = 0.f;
-          ok &= wave_take(a.xs + (size_t)jj * nr2 + e, epoch, &ys);
-          const float ds = a.d[(long long)jj * g.NRP + e];
-          y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, ds), ys));
-        }
-        if (kk > 0) {
-          const float aik = __double2float_rn(-__dmul_rn(c17, dpi_km1));
-          float yk = yk_in, dk = dk_in;
-          if (kl == 0) {
-            ok &= wave_take(ck + e, epoch, &yk);
-            dk = pd[e - plane];
-          }
-          y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dk), yk));
-        }
-        if (jj > 0) {
-          const double u2 = __dmul_rn(drh, dph_k);
-          const float aik = __double2float_rn(-__dmul_rn(__dmul_rn(u2, st_jm1), dti_jm1));
-          float yj = yj_in, dj = dj_in;
-          if (jl == 0) {
-            ok &= wave_take(cj + e, epoch, &yj);
-            dj = pd[e - g.NRP];
-          }
-          y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dj), yj));
-        }
-        if (e > 0) {
-          const float aik = __double2float_rn(-__dmul_rn(__dmul_rn(v, sh_r2[e]), sh_dri[e]));
-          y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dprev), yprev));
-        }
-        pout[e] = y;
-        if (pub_j) wave_publish(pj + e, epoch, y);
-        if (pub_k) wave_publish(pk + e, epoch, y);
-        if (pub_s) wave_publish(xs + e, epoch, y);
-        yprev = y;
-        dprev = d_e;
-      }
-    }
-    if (__any_sync(0xffffffffu, !ok)) return false;
-  }
-  return true;
-}
-
-// Backward solve of one tile: z = (y - sum_{upper} a z) * dinv, lusol's row
-// order [i+1, j+1, k+1, seam].  Mirror image of the forward tile.
-__device__ __forceinline__ bool wave_tile_backward(const WaveArgs &a, const double *sh, unsigned epoch, int tj,
-                                                   int tk, int lane) {
-  const Geo &g = a.g;
-  const DevMesh &m = a.m;
-  const int jl = lane & 3, kl = lane >> 2;
-  const int jj = tj * WJ + jl, kk = tk * WK + kl;
-  const bool valid = jj < g.ntm2 && kk < g.npm2;
-  const int sk = (WJ - 1 - jl) + (WK - 1 - kl);
-  const int nr2 = g.nrm2;
-  const double *sh_drh = sh, *sh_r2 = sh + nr2, *sh_dri = sh + 2 * nr2;
-  double dth_j = 0, sthi_j = 0, dpi_km1 = 0, dpi_k = 0, dph_k = 0, st_j = 0, dti_j = 0, v = 0;
+  const long long row = (long long)(valid ? jj : 0) * g.NRP + (valid ? e : 0);
+  // neighbour tiles across the faces this tile consumes and produces
+  const int te_in = FWD ? te - 1 : te + 1, tj_in = FWD ? tj - 1 : tj + 1;
+  const int te_out = FWD ? te + 1 : te - 1, tj_out = FWD ? tj + 1 : tj - 1;
+  const bool has_in_e = te_in >= 0 && te_in < a.nte, has_in_j = tj_in >= 0 && tj_in < a.ntj;
+  const bool pub_e = valid && (FWD ? el == WE - 1 : el == 0) && te_out >= 0 && te_out < a.nte;
+  const bool pub_j = valid && (FWD ? jl == WJT - 1 : jl == 0) && tj_out >= 0 && tj_out < a.ntj;
+  const bool ext_e = FWD ? el == 0 : el == WE - 1;    // e-neighbour across the face
+  const bool ext_j = FWD ? jl == 0 : jl == WJT - 1;   // j-neighbour across the face
+  const bool cpl_e = valid && (FWD ? e > 0 : e < g.nrm2 - 1);
+  const bool cpl_j = valid && (FWD ? jj > 0 : jj < g.ntm2 - 1);
+  unsigned long long *xe_out = a.xe + (size_t)(tj * a.nte + te) * a.ndiag * 16;
+  unsigned long long *xj_out = a.xj + (size_t)(tj * a.nte + te) * a.ndiag * 16;
+  // per-line constants of the coefficients (load_matrix_pot3d_solve's operand order)
+  double drh = 0, c17 = 0, sd = 0, stj = 0, dtij = 0, r2i = 0, drii = 0;
   if (valid) {
-    const int j = jj + 2, k = kk + 2;
-    dth_j = m.dth[j];
-    sthi_j = m.sth_i[j];
-    dpi_km1 = m.dp_i[k - 1];
-    dpi_k = m.dp_i[k];
-    dph_k = m.dph[k];
-    st_j = m.st[j];
-    dti_j = m.dt_i[j];
-    v = __dmul_rn(__dmul_rn(m.sth[j], dth_j), dph_k);
+    const int i = e + 2, j = jj + 2;
+    drh = m.drh[i];
+    c17 = __dmul_rn(__dmul_rn(drh, m.dth[j]), m.sth_i[j]);
+    sd = __dmul_rn(m.sth[j], m.dth[j]);
+    stj = FWD ? m.st[j - 1] : m.st[j];
+    dtij = FWD ? m.dt_i[j - 1] : m.dt_i[j];
+    r2i = FWD ? m.r2[i - 1] : m.r2[i];
+    drii = FWD ? m.dr_i[i - 1] : m.dr_i[i];
   }
-  const long long base = valid ? ((long long)kk * g.ntm2 + jj) * g.NRP : 0;
-  const bool up_j = valid && jj < g.ntm2 - 1, up_k = valid && kk < g.npm2 - 1;
-  const bool use_seam = valid && kk == 0;
-  const bool pub_j = valid && jl == 0 && tj > 0;
-  const bool pub_k = valid && kl == 0 && tk > 0;
-  const bool pub_s = valid && kk == g.npm2 - 1;
-  const unsigned long long *cj = tj + 1 < a.ntj ? a.xj + ((size_t)(tk * a.ntj + tj + 1) * WK + kl) * nr2 : a.xj;
-  const unsigned long long *ck = tk + 1 < a.ntk ? a.xk + ((size_t)((tk + 1) * a.ntj + tj) * WJ + jl) * nr2 : a.xk;
-  unsigned long long *pj = a.xj + ((size_t)(tk * a.ntj + tj) * WK + kl) * nr2;
-  unsigned long long *pk = a.xk + ((size_t)(tk * a.ntj + tj) * WJ + jl) * nr2;
-  unsigned long long *xs = a.xs + (size_t)jj * nr2;
-  const float *pin = a.in + base, *pdi = a.d + base;
-  float *pout = a.out + base;
-  float ybuf[WAVE_PF], dbuf[WAVE_PF];
-#pragma unroll
-  for (int u = 0; u < WAVE_PF; u++) {
-    const int e = nr2 - 1 - (u - sk);
-    const bool ld = valid && e >= 0 && e < nr2;
-    ybuf[u] = ld ? pin[e] : 0.f;
-    dbuf[u] = ld ? pdi[e] : 0.f;
-  }
-  float zprev = 0.f;
-  bool ok = true;
-  const int nsteps = nr2 + (WJ - 1) + (WK - 1);
-  for (int t0 = 0; t0 < nsteps; t0 += WAVE_PF) {
-#pragma unroll
-    for (int u = 0; u < WAVE_PF; u++) {
-      const int t = t0 + u;
-      const float zj_in = __shfl_down_sync(0xffffffffu, zprev, 1);
-      const float zk_in = __shfl_down_sync(0xffffffffu, zprev, WJ);
-      const int e = nr2 - 1 - (t - sk);
-      const float y_e = ybuf[u], di_e = dbuf[u];
-      {
-        const int ef = e - WAVE_PF;
-        const bool ld = valid && ef >= 0 && ef < nr2;
-        ybuf[u] = ld ? pin[ef] : 0.f;
-        dbuf[u] = ld ? pdi[ef] : 0.f;
-      }
-      if (t < nsteps && valid && e >= 0 && e < nr2) {
-        const double drh = sh_drh[e];
-        float z = y_e;
-        if (e < nr2 - 1) {
-          const float aij = __double2float_rn(-__dmul_rn(__dmul_rn(v, sh_r2[e]), sh_dri[e]));
-          z = __fsub_rn(z, __fmul_rn(aij, zprev));
-        }
-        if (up_j) {
-          const double u2 = __dmul_rn(drh, dph_k);
-          const float aij = __double2float_rn(-__dmul_rn(__dmul_rn(u2, st_j), dti_j));
-          float zj = zj_in;
-          if (jl == WJ - 1) ok &= wave_take(cj + e, epoch, &zj);
-          z = __fsub_rn(z, __fmul_rn(aij, zj));
-        }
-        const double c17 = __dmul_rn(__dmul_rn(drh, dth_j), sthi_j);
-        if (up_k) {
-          const float aij = __double2float_rn(-__dmul_rn(c17, dpi_k));
-          float zk = zk_in;
-          if (kl == WK - 1) ok &= wave_take(ck + e, epoch, &zk);
-          z = __fsub_rn(z, __fmul_rn(aij, zk));
-        }
-        if (use_seam) {
-          const float aij = __double2float_rn(-__dmul_rn(c17, dpi_km1));
-          float zs = 0.f;
-          ok &= wave_take(a.xs + (size_t)jj * nr2 + e, epoch, &zs);
-          z = __fsub_rn(z, __fmul_rn(aij, zs));
-        }
-        z = __fmul_rn(z, di_e);
-        pout[e] = z;
-        if (pub_j) wave_publish(pj + e, epoch, z);
-        if (pub_k) wave_publish(pk + e, epoch, z);
-        if (pub_s) wave_publish(xs + e, epoch, z);
-        zprev = z;
-      }
+  // exchange slot of this thread: who consumes it, which word it is
+  int xf, xs, xl;
+  wave_slot(T, &xf, &xs, &xl);
+  const bool x_tile = xf == 0 ? has_in_e : has_in_j;
+  const unsigned long long *x_src =
+      xf == 0 ? a.xe + (size_t)(tj * a.nte + (x_tile ? te_in : te)) * a.ndiag * 16
+              : a.xj + (size_t)((x_tile ? tj_in : tj) * a.nte + te) * a.ndiag * 16;
+  // the consumer of slot (xf, *, xl): thread (el_c, jl_c) of this tile
+  const int el_c = xf == 0 ? (FWD ? 0 : WE - 1) : xl, jl_c = xf == 0 ? xl : (FWD ? 0 : WJT - 1);
+  const int e_c = te * WE + el_c, jj_c = tj * WJT + jl_c;
+  const int sk_c = FWD ? el_c + jl_c : (WE - 1 - el_c) + (WJT - 1 - jl_c);
+  const bool x_line = x_tile && e_c < g.nrm2 && jj_c < g.ntm2;
+  // the neighbour point across the face (forward: its pivot is needed)
+  const int e_n = xf == 0 ? e_c + (FWD ? -1 : 1) : e_c, jj_n = xf == 1 ? jj_c + (FWD ? -1 : 1) : jj_c;
+  auto x_needed = [&](int t) {
+    const int q = t - sk_c;
+    return x_line && t < a.ndiag && q >= 0 && q < npm2;
+  };
+  auto x_kk = [&](int t) { return FWD ? t - sk_c : npm2 - 1 - (t - sk_c); };
+  unsigned long long xw = 0;  // word of the next chunk
+  float xd = 0.f;             // forward: neighbour pivot of the next chunk
+  auto x_fetch = [&](int c) {
+    const int t = c * WCH + xs;
+    if (x_needed(t)) {
+      xw = wave_load(x_src + (size_t)t * 16 + xl);
+      if (FWD) xd = a.dfac[(long long)x_kk(t) * plane + (long long)jj_n * g.NRP + e_n];
     }
-    if (__any_sync(0xffffffffu, !ok)) return false;
+  };
+  // Commit the fetched chunk c into ring slot c & 1; false on a timeout.
+  auto x_commit = [&](int c) {
+    const int t = c * WCH + xs;
+    bool ok = true;
+    if (x_needed(t)) {
+      unsigned it = 0;
+      while ((unsigned)(xw >> 32) != epoch) {
+        if (++it > WAVE_SPIN_LIMIT) {
+          ok = false;
+          break;
+        }
+        if (it > 8) __nanosleep(32);
+        xw = wave_load(x_src + (size_t)t * 16 + xl);
+      }
+      S.ring[c & 1][xf][xs][xl] = __uint_as_float((unsigned)xw);
+      if (FWD) S.dring[c & 1][xf][xs][xl] = xd;
+    }
+    return ok;
+  };
+
+  const float *pin = a.in + row, *pdd = a.d + row;
+  float *pout = a.out + row;
+  auto kk_of = [&](int t) { return FWD ? t - sk : npm2 - 1 - (t - sk); };
+  auto active = [&](int t) { return valid && t - sk >= 0 && t - sk < npm2; };
+  float ib[WPF], db[WPF];
+#pragma unroll
+  for (int u = 0; u < WPF; u++) {
+    const bool ld = active(u);
+    ib[u] = ld ? pin[kk_of(u) * plane] : 0.f;
+    db[u] = ld ? pdd[kk_of(u) * plane] : 0.f;
+  }
+  float seam_y = 0.f, seam_d = 0.f;  // value (and pivot) at the line's first plane of the sweep
+  float prev = 0.f, dprev = 0.f;     // own value and pivot at the previous step
+  const int nsteps = npm2 + WSK;
+  const int nch = (nsteps + WCH - 1) / WCH;
+  x_fetch(0);
+  bool ok = x_commit(0);
+  x_fetch(1);
+  if (!ok) S.abort = 1;
+  __syncthreads();
+  if (S.abort) return false;
+  for (int c = 0; c < nch; c++) {
+    if (c > 0) {
+      ok = x_commit(c);
+      x_fetch(c + 1);
+      if (!ok) S.abort = 1;
+      __syncthreads();
+      if (S.abort) return false;
+    }
+#pragma unroll
+    for (int u = 0; u < WCH; u++) {
+      const int t = c * WCH + u;
+      const int p = (t + 1) & 1;  // buffer of step t-1
+      const float v_in = ib[u % WPF], d_own = db[u % WPF];
+      {  // prefetch the point WPF steps ahead
+        const int tf = t + WPF;
+        const bool ld = active(tf);
+        ib[u % WPF] = ld ? pin[kk_of(tf) * plane] : 0.f;
+        db[u % WPF] = ld ? pdd[kk_of(tf) * plane] : 0.f;
+      }
+      if (active(t)) {
+        const int kk = kk_of(t);
+        const int K = kk + 2;
+        float ne, nj, dne = 0.f, dnj = 0.f;
+        if (ext_e) {
+          ne = S.ring[c & 1][0][u][jl];
+          if (FWD) dne = S.dring[c & 1][0][u][jl];
+        } else {
+          ne = S.y[p][jl][FWD ? el - 1 : el + 1];
+          if (FWD) dne = S.dv[p][jl][el - 1];
+        }
+        if (ext_j) {
+          nj = S.ring[c & 1][1][u][el];
+          if (FWD) dnj = S.dring[c & 1][1][u][el];
+        } else {
+          nj = S.y[p][FWD ? jl - 1 : jl + 1][el];
+          if (FWD) dnj = S.dv[p][jl - 1][el];
+        }
+        const double dphk = kdph[K];
+        const double u2 = __dmul_rn(drh, dphk);
+        const double v = __dmul_rn(sd, dphk);
+        float y;
+        if (FWD) {
+          // y = r - [seam] - (a1/d) y(k-1) - (a2/d) y(j-1) - (a3/d) y(e-1)
+          y = v_in;
+          if (kk == npm2 - 1) {
+            const float aik = __double2float_rn(-__dmul_rn(c17, kdpi[K]));
+            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, seam_d), seam_y));
+          }
+          if (kk > 0) {
+            const float aik = __double2float_rn(-__dmul_rn(c17, kdpi[K - 1]));
+            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dprev), prev));
+          }
+          if (cpl_j) {
+            const float aik = __double2float_rn(-__dmul_rn(__dmul_rn(u2, stj), dtij));
+            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dnj), nj));
+          }
+          if (cpl_e) {
+            const float aik = __double2float_rn(-__dmul_rn(__dmul_rn(v, r2i), drii));
+            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dne), ne));
+          }
+          if (kk == 0) {
+            seam_y = y;
+            seam_d = d_own;
+          }
+          S.dv[t & 1][jl][el] = d_own;
+        } else {
+          // z = (y - a5 z(e+1) - a6 z(j+1) - a7 z(k+1) - [seam]) * dinv
+          y = v_in;
+          if (cpl_e) {
+            const float aij = __double2float_rn(-__dmul_rn(__dmul_rn(v, r2i), drii));
+            y = __fsub_rn(y, __fmul_rn(aij, ne));
+          }
+          if (cpl_j) {
+            const float aij = __double2float_rn(-__dmul_rn(__dmul_rn(u2, stj), dtij));
+            y = __fsub_rn(y, __fmul_rn(aij, nj));
+          }
+          if (kk < npm2 - 1) {
+            const float aij = __double2float_rn(-__dmul_rn(c17, kdpi[K]));
+            y = __fsub_rn(y, __fmul_rn(aij, prev));
+          }
+          if (kk == 0) {
+            const float aij = __double2float_rn(-__dmul_rn(c17, kdpi[K - 1]));
+            y = __fsub_rn(y, __fmul_rn(aij, seam_y));
+          }
+          y = __fmul_rn(y, d_own);
+          if (kk == npm2 - 1) seam_y = y;
+        }
+        S.y[t & 1][jl][el] = y;
+        pout[(long long)kk * plane] = y;
+        if (pub_e) wave_publish(xe_out + (size_t)(t - (WE - 1)) * 16 + jl, epoch, y);
+        if (pub_j) wave_publish(xj_out + (size_t)(t - (WJT - 1)) * 16 + el, epoch, y);
+        prev = y;
+        dprev = d_own;
+      }
+      __syncthreads();
+    }
   }
   return true;
 }
 
 template <bool FWD>
 __global__ void __launch_bounds__(WAVE_THREADS) k_dilu_wave(WaveArgs a) {
-  extern __shared__ double wave_sh[];  // drh(i), r2(i-1|i), dr_i(i-1|i) for the block's radial points
+  extern __shared__ double wave_k[];  // dph(K), dp_i(K) for K = 0..np
+  __shared__ WaveSmem S;
   const Geo &g = a.g;
-  for (int e = threadIdx.x; e < g.nrm2; e += blockDim.x) {
-    const int i = e + 2;
-    wave_sh[e] = a.m.drh[i];
-    wave_sh[g.nrm2 + e] = FWD ? a.m.r2[i - 1] : a.m.r2[i];
-    wave_sh[2 * g.nrm2 + e] = FWD ? a.m.dr_i[i - 1] : a.m.dr_i[i];
+  double *kdph = wave_k, *kdpi = wave_k + (g.np + 1);
+  for (int K = threadIdx.x; K <= g.np; K += blockDim.x) {
+    kdph[K] = K >= 1 ? a.m.dph[K] : 0.0;
+    kdpi[K] = K >= 1 ? a.m.dp_i[K] : 0.0;
   }
+  if (threadIdx.x == 0) S.abort = 0;
   __syncthreads();
-  const int lane = threadIdx.x & 31;
   const unsigned epoch = *(volatile unsigned *)&a.ctl->epoch;
-  bool run = !(a.check && *(volatile int *)&a.st->status != ST_RUNNING);
+  const bool run = !(a.check && *(volatile int *)&a.st->status != ST_RUNNING);
   while (run) {
-    unsigned t = 0;
-    if (lane == 0) t = atomicAdd(&a.ctl->ticket, 1u);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= (unsigned)a.ntiles) break;
-    const int2 tile = a.order[FWD ? t : a.ntiles - 1 - t];
-    const bool ok = FWD ? wave_tile_forward(a, wave_sh, epoch, tile.x, tile.y, lane)
-                        : wave_tile_backward(a, wave_sh, epoch, tile.x, tile.y, lane);
-    if (!ok) {
-      if (lane == 0) {
+    if (threadIdx.x == 0) {
+      const unsigned t = atomicAdd(&a.ctl->ticket, 1u);
+      S.tile = t < (unsigned)a.ntiles ? a.order[FWD ? t : a.ntiles - 1 - t] : make_int2(-1, -1);
+    }
+    __syncthreads();
+    const int2 tile = S.tile;
+    if (tile.x < 0) break;
+    if (!wave_tile<FWD>(a, S, kdph, kdpi, epoch, tile.x, tile.y)) {
+      if (threadIdx.x == 0) {
         atomicExch(&a.ctl->error, 1);
         if (a.st) atomicExch(&a.st->status, ST_TIMEOUT);
       }
-      run = false;
+      break;
     }
   }
-  __syncwarp();
-  if (lane == 0) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
     __threadfence();
-    const unsigned total = gridDim.x * (blockDim.x / 32);
-    if (atomicAdd(&a.ctl->done, 1u) == total - 1) {  // last warp: reset for the next sweep
+    if (atomicAdd(&a.ctl->done, 1u) == gridDim.x - 1) {  // last block: reset for the next sweep
       atomicExch(&a.ctl->ticket, 0u);
       atomicExch(&a.ctl->done, 0u);
       __threadfence();
       atomicAdd(&a.ctl->epoch, 1u);
     }
   }
+}
+
+__global__ void k_narrow_rhs(long long n, const double *__restrict__ b, float *__restrict__ r32) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    r32[t] = (float)b[t];
 }
 
 __global__ void k_wave_reset(WaveCtl *c) {
@@ -436,10 +458,10 @@ struct DiluState {
   int nlev = 0;
   std::vector<int> kk_lo, nkk, nblk;  // per level launch shape (factorisation)
   // wavefront sweeps
-  unsigned long long *xj = nullptr, *xk = nullptr, *xs = nullptr;
+  unsigned long long *xe = nullptr, *xj = nullptr;
   int2 *order = nullptr;
   WaveCtl *ctl = nullptr;
-  int ntj = 0, ntk = 0, ntiles = 0, wave_blocks = 0;
+  int nte = 0, ntj = 0, ntiles = 0, ndiag = 0, wave_blocks = 0;
   size_t wave_smem = 0;
 };
 
@@ -470,34 +492,35 @@ static void launch_factor_level(Solver *s, int l) {
 static int wave_setup(Solver *s) {
   DiluState *D = s->dilu;
   const Geo &g = s->g;
-  D->ntj = (g.ntm2 + WJ - 1) / WJ;
-  D->ntk = (g.npm2 + WK - 1) / WK;
-  D->ntiles = D->ntj * D->ntk;
-  const size_t nxj = (size_t)D->ntiles * WK * g.nrm2, nxk = (size_t)D->ntiles * WJ * g.nrm2,
-               nxs = (size_t)g.ntm2 * g.nrm2;
+  D->nte = (g.nrm2 + WE - 1) / WE;
+  D->ntj = (g.ntm2 + WJT - 1) / WJT;
+  D->ntiles = D->nte * D->ntj;
+  D->ndiag = g.npm2 + 16;
+  const size_t nx = (size_t)D->ntiles * D->ndiag * 16;
   int st;
-  if ((st = s->alloc((void **)&D->xj, 8 * nxj)) || (st = s->alloc((void **)&D->xk, 8 * nxk)) ||
-      (st = s->alloc((void **)&D->xs, 8 * nxs)) || (st = s->alloc((void **)&D->order, sizeof(int2) * D->ntiles)) ||
+  if ((st = s->alloc((void **)&D->xe, 8 * nx)) || (st = s->alloc((void **)&D->xj, 8 * nx)) ||
+      (st = s->alloc((void **)&D->order, sizeof(int2) * D->ntiles)) ||
       (st = s->alloc((void **)&D->ctl, sizeof(WaveCtl))))
     return st;
-  // Tickets in order of the tile's first wavefront step 4 tj + 8 tk (ties by
-  // tj): every producer of a tile (tj-1, tk), (tj, tk-1) and, through the
-  // seam, (tj, 0) has a smaller key.
+  // Tickets in order of the tile's first wavefront step WE te + WJT tj
+  // (ties by te): a tile's producers (te-1, tj) and (te, tj-1) have smaller
+  // keys; the backward sweep takes the tickets in reverse.
   std::vector<int2> ord;
   ord.reserve(D->ntiles);
-  for (int tk = 0; tk < D->ntk; tk++)
-    for (int tj = 0; tj < D->ntj; tj++) ord.push_back(make_int2(tj, tk));
+  for (int tj = 0; tj < D->ntj; tj++)
+    for (int te = 0; te < D->nte; te++) ord.push_back(make_int2(te, tj));
   std::stable_sort(ord.begin(), ord.end(), [](const int2 &x, const int2 &y) {
-    const int kx = WJ * x.x + WK * x.y, ky = WJ * y.x + WK * y.y;
+    const int kx = WE * x.x + WJT * x.y, ky = WE * y.x + WJT * y.y;
     return kx != ky ? kx < ky : x.x < y.x;
   });
   CK(cudaMemcpyAsync(D->order, ord.data(), sizeof(int2) * D->ntiles, cudaMemcpyHostToDevice, s->stream));
-  CK(cudaMemsetAsync(D->xj, 0, 8 * nxj, s->stream));
-  CK(cudaMemsetAsync(D->xk, 0, 8 * nxk, s->stream));
-  CK(cudaMemsetAsync(D->xs, 0, 8 * nxs, s->stream));
-  CK(cudaMemsetAsync(D->ctl, 0, sizeof(WaveCtl), s->stream));
-  D->wave_smem = sizeof(double) * 3 * g.nrm2;
-  if (D->wave_smem > 48 * 1024) {
+  CK(cudaMemsetAsync(D->xe, 0, 8 * nx, s->stream));
+  CK(cudaMemsetAsync(D->xj, 0, 8 * nx, s->stream));
+  const WaveCtl c0{0u, 0u, 1u, 0};  // tag 0 is the zeroed buffers': sweeps start at 1
+  CK(cudaMemcpyAsync(D->ctl, &c0, sizeof(WaveCtl), cudaMemcpyHostToDevice, s->stream));
+  D->wave_smem = sizeof(double) * 2 * (g.np + 1);
+  const size_t smem_total = D->wave_smem + sizeof(WaveSmem);
+  if (smem_total > 48 * 1024) {
     CK(cudaFuncSetAttribute(k_dilu_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem));
     CK(cudaFuncSetAttribute(k_dilu_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem));
   }
@@ -506,8 +529,7 @@ static int wave_setup(Solver *s) {
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_THREADS, D->wave_smem));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_THREADS, D->wave_smem));
-  const int warps = std::max(1, std::min(occ_f, occ_b)) * nsm * (WAVE_THREADS / 32);
-  D->wave_blocks = std::max(1, std::min(warps, D->ntiles) / (WAVE_THREADS / 32));
+  D->wave_blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, D->ntiles));
   return POT3D_OK;
 }
 
@@ -519,16 +541,17 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   a.in = fwd ? D->r32 : D->y32;
   a.out = fwd ? D->y32 : D->z32;
   a.d = fwd ? D->d : D->dinv;
+  a.dfac = D->d;
+  a.xe = D->xe;
   a.xj = D->xj;
-  a.xk = D->xk;
-  a.xs = D->xs;
   a.order = D->order;
   a.ctl = D->ctl;
   a.st = s->d_state;
   a.check = check ? 1 : 0;
+  a.nte = D->nte;
   a.ntj = D->ntj;
-  a.ntk = D->ntk;
   a.ntiles = D->ntiles;
+  a.ndiag = D->ndiag;
   if (fwd)
     k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS, D->wave_smem, s->stream>>>(a);
   else
@@ -586,6 +609,33 @@ int dilu_sweeps(Solver *s, bool check_status) {
   launch_wave(s, true, check_status);
   launch_wave(s, false, check_status);
   return pot3d_cuda_status(cudaGetLastError(), "ILU(0) sweeps");
+}
+
+// Average device time of the forward and of the backward sweep over `reps`
+// applications to the FP32 right-hand side.
+int dilu_time(Solver *s, int reps, double ms[2]) {
+  DiluState *D = s->dilu;
+  int st;
+  if ((st = dilu_reset(s))) return st;
+  k_narrow_rhs<<<grid1d(s->g.Np), NTHR, 0, s->stream>>>(s->g.Np, s->d_b, D->r32);
+  cudaEvent_t e[3];
+  for (auto &x : e) CK(cudaEventCreate(&x));
+  ms[0] = ms[1] = 0.0;
+  for (int it = 0; it < reps; it++) {
+    CK(cudaEventRecord(e[0], s->stream));
+    launch_wave(s, true, false);
+    CK(cudaEventRecord(e[1], s->stream));
+    launch_wave(s, false, false);
+    CK(cudaEventRecord(e[2], s->stream));
+    CK(cudaEventSynchronize(e[2]));
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, e[0], e[1]);
+    cudaEventElapsedTime(&b, e[1], e[2]);
+    ms[0] += a / reps;
+    ms[1] += b / reps;
+  }
+  for (auto &x : e) cudaEventDestroy(x);
+  return dilu_status(s);
 }
 
 // Status of the sweeps issued so far (synchronises the solver stream).

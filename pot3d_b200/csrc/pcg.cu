@@ -2109,14 +2109,14 @@ extern "C" int pot3d_gpu_batch_solve(pot3d_gpu_batch *h, int ncgmax, double epsc
   // Loop: run 2U iterations of the running cases from a graph, read their
   // states, drop the finished ones from the table (so later launches cover
   // only running cases' tiles) and re-capture when the set changed.
-  int last_total = -1, stalls = 0;
+  long long last_total = -1;
+  int stalls = 0;
   for (;;) {
     std::vector<int> run;
-    int total = 0;
-    for (int q : B.act) {
+    long long total = 0;  // iterations of all cases, finished ones included
+    for (int q : B.act)
       if (B.pin[q].status == ST_RUNNING) run.push_back(q);
-      total += B.pin[q].ncg;
-    }
+    for (int q = 0; q < n; q++) total += B.pin[q].ncg;
     if (run.empty()) break;
     if (total <= last_total) {
       if (++stalls >= 3) {

@@ -91,7 +91,8 @@ float *dilu_z32(Solver *s);   // FP32 output z = (LU)^-1 r32
 // kernels return at once when the PCG state is no longer running.
 int dilu_sweeps(Solver *s, bool check_status);
 int dilu_reset(Solver *s);
-int dilu_status(Solver *s);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
+int dilu_status(Solver *s);
+int dilu_time(Solver *s, int reps, double ms[2]);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
 int dilu_diag(Solver *s, float *d_host, float *dinv_host);
 int dilu_sweep_launches(Solver *s);
 

@@ -112,6 +112,12 @@ class Pot3dSolver:
     def prec_dev(self, x):
         check(_lib.lib().pot3d_gpu_prec_dev(self._h, C.c_void_p(x.data_ptr())))
 
+    def time_sweeps(self, reps: int = 10):
+        """(forward ms, backward ms) of the ILU(0) wavefront sweeps (ifprec=2)."""
+        ms = np.zeros(2)
+        check(_lib.lib().pot3d_gpu_time_sweeps(self._h, reps, dptr(ms)))
+        return float(ms[0]), float(ms[1])
+
     def time_kernels(self, reps: int = 20):
         """Average ms per launch of the stencil and update kernels, and their
         algorithmic DRAM bytes per launch."""
