@@ -121,30 +121,42 @@ __global__ void k_dilu_factor(LevelArgs a) {
 // (el-1, jl) and (el, jl-1) one step earlier: the block runs in lockstep,
 // one barrier per step, and exchanges them through shared memory.
 //
-// Across tile faces values travel as 64-bit words holding the FP32 value
-// and a sweep tag.  A word is indexed by the step at which its consumer
-// needs it, so the words of one face for 8 consecutive steps are one
-// contiguous block; the whole block fetches the next 8 steps' words (and,
-// forward, the neighbour pivots) one chunk ahead, checks their tags when
-// the chunk starts and polls again (bounded) only for words not yet
-// written.  Tiles are taken in the order of the tickets of a global
-// counter, sorted so that every tile's producers (e-1 and j-1 faces)
-// hold smaller tickets: a block only ever waits for a tile already owned
-// by a running block, and the kernel needs no co-residency.  The last
-// block to finish resets the counter and advances the tag.
+// Memory traffic stays coalesced despite the skew:
+//  * the sweep's private streams (coefficients, the intermediate y) are
+//    stored in a tile-skewed layout [tile][step][thread], so one step of a
+//    block is one contiguous 1 KB run per float;
+//  * the padded-layout vectors shared with the other kernels (r32 in,
+//    z32 out) go through a ring of phi planes in shared memory: every
+//    thread loads (or stores) its own line of plane p at the same step, so
+//    each warp touches two 64-byte row segments, and reads (or writes) its
+//    ring entry at its skewed step.
 //
-// Every value is computed with the operations, and in the order, of the
-// reference's lusol (src/pot3d.F90:5227-5302), so the sweeps are
-// bit-identical to it.
+// Across tile faces values travel as 64-bit words holding the FP32 value
+// and a sweep tag, indexed by the step at which the consumer needs them, so
+// the words of one face for 8 consecutive steps are one contiguous block;
+// the block fetches the next 8 steps' words one chunk ahead, one thread per
+// face waits for the chunk's last word and the others re-poll (bounded)
+// only words not yet visible.  Tiles are taken in the order of the tickets
+// of a global counter, sorted so that every tile's producers hold smaller
+// tickets: a block only waits for a tile owned by a running block, and the
+// kernel needs no co-residency.  The last block to finish resets the
+// counter and advances the tag.
+//
+// The FP32 coefficients are formed once, after the factorisation, with the
+// reference's operations (lusol's l = a/d of the lower entries and the FP32
+// upper entries, src/pot3d.F90:5227-5302) and applied in lusol's order, so
+// the sweeps are bit-identical to it.
 // ============================================================================
 constexpr int WE = 16, WJT = 16;        // lines per tile in e and j
 constexpr int WAVE_THREADS = WE * WJT;  // one thread per line
 constexpr int WCH = 8;                  // steps per exchange chunk
-constexpr int WPF = 4;                  // prefetch distance of the point loads (steps)
+constexpr int WPF = 8;                  // prefetch distance of the streams (steps, power of 2)
 constexpr int WSK = (WE - 1) + (WJT - 1);
+constexpr int WRIN = WSK + 1 + WPF;     // input plane ring (forward r32)
+constexpr int WROUT = 32;               // output plane ring (backward z32), > WSK
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
 static_assert(2 * WCH * 16 == WAVE_THREADS, "one exchange word per thread and chunk");
-static_assert(WCH % WPF == 0, "chunk is a whole number of prefetch rounds");
+static_assert(WROUT > WSK, "a plane is flushed after its last line wrote it");
 
 struct WaveCtl {
   unsigned ticket, done, epoch;
@@ -153,17 +165,19 @@ struct WaveCtl {
 
 struct WaveArgs {
   Geo g;
-  DevMesh m;
-  const float *in;    // forward: r32 ; backward: y32
-  float *out;         // forward: y32 ; backward: z32
-  const float *d;     // forward: factor diagonal d ; backward: dinv
-  const float *dfac;  // factor diagonal d (forward neighbour pivots)
+  const float *r32;      // forward input (padded layout)
+  float *z32;            // backward output (padded layout)
+  float *ys;             // intermediate y (tile-skewed, forward step order)
+  const float *lf;       // forward coefficients (tile-skewed, [c][thread], c = l_k, l_j, l_e)
+  const float4 *ub;      // backward coefficients (tile-skewed): u_e, u_j, u_k, dinv
+  const float *seam_f;   // forward seam coefficient of the last plane, per line
+  const float *seam_b;   // backward seam coupling of the first plane, per line
   unsigned long long *xe, *xj;  // e-face and j-face exchange words
-  const int2 *order;  // ticket -> tile (te, tj) in forward order
+  const int2 *order;     // ticket -> tile (te, tj) in forward order
   WaveCtl *ctl;
   SolveState *st;
-  int check;          // skip when the solve state is no longer running
-  int nte, ntj, ntiles, ndiag;
+  int check;             // skip when the solve state is no longer running
+  int nte, ntj, ntiles, ndiag, nsteps;
 };
 
 __device__ __forceinline__ void wave_publish(unsigned long long *p, unsigned epoch, float v) {
@@ -176,27 +190,54 @@ __device__ __forceinline__ unsigned long long wave_load(const unsigned long long
   return w;
 }
 
-struct WaveSmem {
+// Asynchronous copies global -> shared (zero-filled when !pred).
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool pred) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(pred ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async16(float4 *dst, const float4 *src, bool pred) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(pred ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+struct WaveSmemF {                   // forward sweep
+  float lf[WPF][3][WAVE_THREADS];    // coefficient stream, slot = step % WPF
+  float rin[WRIN][WAVE_THREADS];     // r32 planes, slot = plane % WRIN
   float y[2][WJT][WE + 1];           // step parity, line values
-  float dv[2][WJT][WE + 1];          // forward: the lines' pivots d at their current point
   float ring[2][2][WCH][16];         // chunk parity, face (0: e, 1: j), step in chunk, line
-  float dring[2][2][WCH][16];        // forward: pivots of the neighbours across the faces
+  int2 tile;
+  int abort;
+};
+struct WaveSmemB {                   // backward sweep
+  float4 ub[WPF][WAVE_THREADS];      // coefficient stream
+  float yin[WPF][WAVE_THREADS];      // y stream
+  float zout[WROUT][WAVE_THREADS];   // z32 planes, slot = plane % WROUT
+  float y[2][WJT][WE + 1];
+  float ring[2][2][WCH][16];
   int2 tile;
   int abort;
 };
 
-// Exchange slot (face, step s of chunk, line) of thread T.
-__device__ __forceinline__ void wave_slot(int T, int *f, int *s, int *line) {
-  *f = T >> 7;
-  *s = (T >> 4) & (WCH - 1);
-  *line = T & 15;
-}
+template <bool FWD>
+struct WaveSmemSel;
+template <>
+struct WaveSmemSel<true> {
+  using type = WaveSmemF;
+};
+template <>
+struct WaveSmemSel<false> {
+  using type = WaveSmemB;
+};
 
 template <bool FWD>
-__device__ __forceinline__ bool wave_tile(const WaveArgs &a, WaveSmem &S, const double *kdph, const double *kdpi,
-                                          unsigned epoch, int te, int tj) {
+__device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S, unsigned epoch,
+                                          int te, int tj) {
   const Geo &g = a.g;
-  const DevMesh &m = a.m;
   const int T = threadIdx.x;
   const int el = T & (WE - 1), jl = T / WE;
   const int e = te * WE + el, jj = tj * WJT + jl;
@@ -205,6 +246,8 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, WaveSmem &S, const 
   const int npm2 = g.npm2;
   const long long plane = (long long)g.ntm2 * g.NRP;
   const long long row = (long long)(valid ? jj : 0) * g.NRP + (valid ? e : 0);
+  const int ti = tj * a.nte + te;
+  const size_t tbase = (size_t)ti * a.nsteps * WAVE_THREADS;  // tile-skewed stream base
   // neighbour tiles across the faces this tile consumes and produces
   const int te_in = FWD ? te - 1 : te + 1, tj_in = FWD ? tj - 1 : tj + 1;
   const int te_out = FWD ? te + 1 : te - 1, tj_out = FWD ? tj + 1 : tj - 1;
@@ -215,199 +258,171 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, WaveSmem &S, const 
   const bool ext_j = FWD ? jl == 0 : jl == WJT - 1;   // j-neighbour across the face
   const bool cpl_e = valid && (FWD ? e > 0 : e < g.nrm2 - 1);
   const bool cpl_j = valid && (FWD ? jj > 0 : jj < g.ntm2 - 1);
-  unsigned long long *xe_out = a.xe + (size_t)(tj * a.nte + te) * a.ndiag * 16;
-  unsigned long long *xj_out = a.xj + (size_t)(tj * a.nte + te) * a.ndiag * 16;
-  // per-line constants of the coefficients (load_matrix_pot3d_solve's operand order)
-  double drh = 0, c17 = 0, sd = 0, stj = 0, dtij = 0, r2i = 0, drii = 0;
-  if (valid) {
-    const int i = e + 2, j = jj + 2;
-    drh = m.drh[i];
-    c17 = __dmul_rn(__dmul_rn(drh, m.dth[j]), m.sth_i[j]);
-    sd = __dmul_rn(m.sth[j], m.dth[j]);
-    stj = FWD ? m.st[j - 1] : m.st[j];
-    dtij = FWD ? m.dt_i[j - 1] : m.dt_i[j];
-    r2i = FWD ? m.r2[i - 1] : m.r2[i];
-    drii = FWD ? m.dr_i[i - 1] : m.dr_i[i];
-  }
-  // exchange slot of this thread: who consumes it, which word it is
-  int xf, xs, xl;
-  wave_slot(T, &xf, &xs, &xl);
+  unsigned long long *xe_out = a.xe + (size_t)ti * a.ndiag * 16;
+  unsigned long long *xj_out = a.xj + (size_t)ti * a.ndiag * 16;
+  const float seam_c = valid ? (FWD ? a.seam_f[row] : a.seam_b[row]) : 0.f;
+  // exchange slot of this thread: face xf, step xs of the chunk, line xl
+  const int xf = T >> 7, xs = (T >> 4) & (WCH - 1), xl = T & 15;
   const bool x_tile = xf == 0 ? has_in_e : has_in_j;
   const unsigned long long *x_src =
       xf == 0 ? a.xe + (size_t)(tj * a.nte + (x_tile ? te_in : te)) * a.ndiag * 16
               : a.xj + (size_t)((x_tile ? tj_in : tj) * a.nte + te) * a.ndiag * 16;
   // the consumer of slot (xf, *, xl): thread (el_c, jl_c) of this tile
   const int el_c = xf == 0 ? (FWD ? 0 : WE - 1) : xl, jl_c = xf == 0 ? xl : (FWD ? 0 : WJT - 1);
-  const int e_c = te * WE + el_c, jj_c = tj * WJT + jl_c;
   const int sk_c = FWD ? el_c + jl_c : (WE - 1 - el_c) + (WJT - 1 - jl_c);
-  const bool x_line = x_tile && e_c < g.nrm2 && jj_c < g.ntm2;
-  // the neighbour point across the face (forward: its pivot is needed)
-  const int e_n = xf == 0 ? e_c + (FWD ? -1 : 1) : e_c, jj_n = xf == 1 ? jj_c + (FWD ? -1 : 1) : jj_c;
+  const bool x_line = x_tile && te * WE + el_c < g.nrm2 && tj * WJT + jl_c < g.ntm2;
   auto x_needed = [&](int t) {
     const int q = t - sk_c;
     return x_line && t < a.ndiag && q >= 0 && q < npm2;
   };
-  auto x_kk = [&](int t) { return FWD ? t - sk_c : npm2 - 1 - (t - sk_c); };
   unsigned long long xw = 0;  // word of the next chunk
-  float xd = 0.f;             // forward: neighbour pivot of the next chunk
   auto x_fetch = [&](int c) {
     const int t = c * WCH + xs;
-    if (x_needed(t)) {
-      xw = wave_load(x_src + (size_t)t * 16 + xl);
-      if (FWD) xd = a.dfac[(long long)x_kk(t) * plane + (long long)jj_n * g.NRP + e_n];
+    if (x_needed(t)) xw = wave_load(x_src + (size_t)t * 16 + xl);
+  };
+  // Poll one word until its tag is current (bounded); false on a timeout.
+  auto x_poll = [&](int t, unsigned long long *w) {
+    unsigned it = 0;
+    while ((unsigned)(*w >> 32) != epoch) {
+      if (++it > WAVE_SPIN_LIMIT) return false;
+      if (it > 4) __nanosleep(it < 64 ? 32 : 256);
+      *w = wave_load(x_src + (size_t)t * 16 + xl);
     }
+    return true;
+  };
+  // One thread per face waits for the chunk's last word of line 0: all
+  // lines of one step are published at the same producer step, so after it
+  // the chunk's other words are (almost always) visible too.
+  auto x_lead = [&](int c) {
+    const int t = c * WCH + xs;
+    if (xs == WCH - 1 && xl == 0 && x_needed(t)) return x_poll(t, &xw);
+    return true;
   };
   // Commit the fetched chunk c into ring slot c & 1; false on a timeout.
   auto x_commit = [&](int c) {
     const int t = c * WCH + xs;
     bool ok = true;
     if (x_needed(t)) {
-      unsigned it = 0;
-      while ((unsigned)(xw >> 32) != epoch) {
-        if (++it > WAVE_SPIN_LIMIT) {
-          ok = false;
-          break;
-        }
-        if (it > 8) __nanosleep(32);
-        xw = wave_load(x_src + (size_t)t * 16 + xl);
-      }
+      if ((unsigned)(xw >> 32) != epoch) xw = wave_load(x_src + (size_t)t * 16 + xl);
+      ok = x_poll(t, &xw);
       S.ring[c & 1][xf][xs][xl] = __uint_as_float((unsigned)xw);
-      if (FWD) S.dring[c & 1][xf][xs][xl] = xd;
     }
     return ok;
   };
 
-  const float *pin = a.in + row, *pdd = a.d + row;
-  float *pout = a.out + row;
   auto kk_of = [&](int t) { return FWD ? t - sk : npm2 - 1 - (t - sk); };
   auto active = [&](int t) { return valid && t - sk >= 0 && t - sk < npm2; };
-  float ib[WPF], db[WPF];
-#pragma unroll
-  for (int u = 0; u < WPF; u++) {
-    const bool ld = active(u);
-    ib[u] = ld ? pin[kk_of(u) * plane] : 0.f;
-    db[u] = ld ? pdd[kk_of(u) * plane] : 0.f;
-  }
-  float seam_y = 0.f, seam_d = 0.f;  // value (and pivot) at the line's first plane of the sweep
-  float prev = 0.f, dprev = 0.f;     // own value and pivot at the previous step
-  const int nsteps = npm2 + WSK;
+  const int nsteps = a.nsteps;
+  // Streams: one copy group per step, issued WPF steps before it is read.
+  // Forward: the coefficients of step t+WPF and this line's r32 of plane
+  // t+WPF (read at the step t+WPF+s that handles it).  Backward: the
+  // coefficients and y of step t+WPF (y in reversed forward step order).
+  auto issue = [&](int t) {
+    const bool in_t = t < nsteps;
+    const size_t so = tbase + (size_t)(in_t ? t : 0) * WAVE_THREADS + T;
+    if constexpr (FWD) {
+      const size_t lo = tbase * 3 + (size_t)(in_t ? t : 0) * 3 * WAVE_THREADS + T;
+      for (int c3 = 0; c3 < 3; c3++) cp_async4(&S.lf[t & (WPF - 1)][c3][T], a.lf + lo + c3 * WAVE_THREADS, in_t);
+      const bool rp = valid && t < npm2;
+      cp_async4(&S.rin[t % WRIN][T], a.r32 + row + (rp ? (long long)t * plane : 0), rp);
+    } else {
+      cp_async16(&S.ub[t & (WPF - 1)][T], a.ub + so, in_t);
+      const size_t yo = tbase + (size_t)(in_t ? nsteps - 1 - t : 0) * WAVE_THREADS + T;
+      cp_async4(&S.yin[t & (WPF - 1)][T], a.ys + yo, in_t);
+    }
+    cp_async_commit();
+  };
+#pragma unroll 1
+  for (int t = 0; t < WPF; t++) issue(t);
+  float seam_y = 0.f;  // value at the line's first plane of the sweep
+  float prev = 0.f;    // own value at the previous step
   const int nch = (nsteps + WCH - 1) / WCH;
+  bool ok = true;
   x_fetch(0);
-  bool ok = x_commit(0);
-  x_fetch(1);
-  if (!ok) S.abort = 1;
-  __syncthreads();
-  if (S.abort) return false;
+#pragma unroll 1
   for (int c = 0; c < nch; c++) {
-    if (c > 0) {
-      ok = x_commit(c);
-      x_fetch(c + 1);
-      if (!ok) S.abort = 1;
-      __syncthreads();
-      if (S.abort) return false;
+    if (!x_lead(c)) S.abort = 1;
+    __syncthreads();
+    ok = x_commit(c);
+    x_fetch(c + 1);
+    if (!ok) S.abort = 1;
+    __syncthreads();
+    if (S.abort) {
+      cp_async_wait<0>();
+      return false;
     }
 #pragma unroll
     for (int u = 0; u < WCH; u++) {
       const int t = c * WCH + u;
       const int p = (t + 1) & 1;  // buffer of step t-1
-      const float v_in = ib[u % WPF], d_own = db[u % WPF];
-      {  // prefetch the point WPF steps ahead
-        const int tf = t + WPF;
-        const bool ld = active(tf);
-        ib[u % WPF] = ld ? pin[kk_of(tf) * plane] : 0.f;
-        db[u % WPF] = ld ? pdd[kk_of(tf) * plane] : 0.f;
+      if constexpr (!FWD) {
+        // flush the z32 plane whose last line was written at step t-1
+        const int kd = npm2 + WSK - t;
+        if (valid && kd >= 0 && kd < npm2 && t > WSK) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
       }
+      cp_async_wait<WPF - 1>();  // this step's group (and every older one) has landed
+      float v_in, c0, c1, c2, c3 = 0.f;
+      if constexpr (FWD) {
+        c0 = S.lf[t & (WPF - 1)][0][T];
+        c1 = S.lf[t & (WPF - 1)][1][T];
+        c2 = S.lf[t & (WPF - 1)][2][T];
+        const int kr = t - sk;
+        v_in = S.rin[(kr >= 0 ? kr : 0) % WRIN][T];
+      } else {
+        const float4 cf = S.ub[t & (WPF - 1)][T];
+        c0 = cf.x;
+        c1 = cf.y;
+        c2 = cf.z;
+        c3 = cf.w;
+        v_in = S.yin[t & (WPF - 1)][T];
+      }
+      issue(t + WPF);
       if (active(t)) {
         const int kk = kk_of(t);
-        const int K = kk + 2;
-        float ne, nj, dne = 0.f, dnj = 0.f;
-        if (ext_e) {
-          ne = S.ring[c & 1][0][u][jl];
-          if (FWD) dne = S.dring[c & 1][0][u][jl];
-        } else {
-          ne = S.y[p][jl][FWD ? el - 1 : el + 1];
-          if (FWD) dne = S.dv[p][jl][el - 1];
-        }
-        if (ext_j) {
-          nj = S.ring[c & 1][1][u][el];
-          if (FWD) dnj = S.dring[c & 1][1][u][el];
-        } else {
-          nj = S.y[p][FWD ? jl - 1 : jl + 1][el];
-          if (FWD) dnj = S.dv[p][jl - 1][el];
-        }
-        const double dphk = kdph[K];
-        const double u2 = __dmul_rn(drh, dphk);
-        const double v = __dmul_rn(sd, dphk);
-        float y;
+        const float ne = ext_e ? S.ring[c & 1][0][u][jl] : S.y[p][jl][FWD ? el - 1 : el + 1];
+        const float nj = ext_j ? S.ring[c & 1][1][u][el] : S.y[p][FWD ? jl - 1 : jl + 1][el];
+        float y = v_in;
         if (FWD) {
-          // y = r - [seam] - (a1/d) y(k-1) - (a2/d) y(j-1) - (a3/d) y(e-1)
-          y = v_in;
-          if (kk == npm2 - 1) {
-            const float aik = __double2float_rn(-__dmul_rn(c17, kdpi[K]));
-            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, seam_d), seam_y));
-          }
-          if (kk > 0) {
-            const float aik = __double2float_rn(-__dmul_rn(c17, kdpi[K - 1]));
-            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dprev), prev));
-          }
-          if (cpl_j) {
-            const float aik = __double2float_rn(-__dmul_rn(__dmul_rn(u2, stj), dtij));
-            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dnj), nj));
-          }
-          if (cpl_e) {
-            const float aik = __double2float_rn(-__dmul_rn(__dmul_rn(v, r2i), drii));
-            y = __fsub_rn(y, __fmul_rn(__fdiv_rn(aik, dne), ne));
-          }
-          if (kk == 0) {
-            seam_y = y;
-            seam_d = d_own;
-          }
-          S.dv[t & 1][jl][el] = d_own;
+          // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1)
+          if (kk == npm2 - 1) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
+          if (kk > 0) y = __fsub_rn(y, __fmul_rn(c0, prev));
+          if (cpl_j) y = __fsub_rn(y, __fmul_rn(c1, nj));
+          if (cpl_e) y = __fsub_rn(y, __fmul_rn(c2, ne));
+          if (kk == 0) seam_y = y;
         } else {
-          // z = (y - a5 z(e+1) - a6 z(j+1) - a7 z(k+1) - [seam]) * dinv
-          y = v_in;
-          if (cpl_e) {
-            const float aij = __double2float_rn(-__dmul_rn(__dmul_rn(v, r2i), drii));
-            y = __fsub_rn(y, __fmul_rn(aij, ne));
-          }
-          if (cpl_j) {
-            const float aij = __double2float_rn(-__dmul_rn(__dmul_rn(u2, stj), dtij));
-            y = __fsub_rn(y, __fmul_rn(aij, nj));
-          }
-          if (kk < npm2 - 1) {
-            const float aij = __double2float_rn(-__dmul_rn(c17, kdpi[K]));
-            y = __fsub_rn(y, __fmul_rn(aij, prev));
-          }
-          if (kk == 0) {
-            const float aij = __double2float_rn(-__dmul_rn(c17, kdpi[K - 1]));
-            y = __fsub_rn(y, __fmul_rn(aij, seam_y));
-          }
-          y = __fmul_rn(y, d_own);
+          // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv
+          if (cpl_e) y = __fsub_rn(y, __fmul_rn(c0, ne));
+          if (cpl_j) y = __fsub_rn(y, __fmul_rn(c1, nj));
+          if (kk < npm2 - 1) y = __fsub_rn(y, __fmul_rn(c2, prev));
+          if (kk == 0) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
+          y = __fmul_rn(y, c3);
           if (kk == npm2 - 1) seam_y = y;
         }
         S.y[t & 1][jl][el] = y;
-        pout[(long long)kk * plane] = y;
+        if constexpr (FWD)
+          a.ys[tbase + (size_t)t * WAVE_THREADS + T] = y;
+        else
+          S.zout[kk % WROUT][T] = y;
         if (pub_e) wave_publish(xe_out + (size_t)(t - (WE - 1)) * 16 + jl, epoch, y);
         if (pub_j) wave_publish(xj_out + (size_t)(t - (WJT - 1)) * 16 + el, epoch, y);
         prev = y;
-        dprev = d_own;
       }
       __syncthreads();
     }
   }
+  if constexpr (!FWD) {  // the first plane completes at the last step
+    const int kd = npm2 + WSK - nsteps;
+    if (valid && kd >= 0 && kd < npm2) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
+  }
+  cp_async_wait<0>();  // the rings are reused by the next tile
   return true;
 }
 
 template <bool FWD>
-__global__ void __launch_bounds__(WAVE_THREADS) k_dilu_wave(WaveArgs a) {
-  extern __shared__ double wave_k[];  // dph(K), dp_i(K) for K = 0..np
-  __shared__ WaveSmem S;
-  const Geo &g = a.g;
-  double *kdph = wave_k, *kdpi = wave_k + (g.np + 1);
-  for (int K = threadIdx.x; K <= g.np; K += blockDim.x) {
-    kdph[K] = K >= 1 ? a.m.dph[K] : 0.0;
-    kdpi[K] = K >= 1 ? a.m.dp_i[K] : 0.0;
-  }
+__global__ void __launch_bounds__(WAVE_THREADS, 3) k_dilu_wave(WaveArgs a) {
+  using Sm = typename WaveSmemSel<FWD>::type;
+  extern __shared__ float4 wave_dyn[];
+  Sm &S = *reinterpret_cast<Sm *>(wave_dyn);
   if (threadIdx.x == 0) S.abort = 0;
   __syncthreads();
   const unsigned epoch = *(volatile unsigned *)&a.ctl->epoch;
@@ -420,13 +435,14 @@ __global__ void __launch_bounds__(WAVE_THREADS) k_dilu_wave(WaveArgs a) {
     __syncthreads();
     const int2 tile = S.tile;
     if (tile.x < 0) break;
-    if (!wave_tile<FWD>(a, S, kdph, kdpi, epoch, tile.x, tile.y)) {
+    if (!wave_tile<FWD>(a, S, epoch, tile.x, tile.y)) {
       if (threadIdx.x == 0) {
         atomicExch(&a.ctl->error, 1);
         if (a.st) atomicExch(&a.st->status, ST_TIMEOUT);
       }
       break;
     }
+    __syncthreads();  // S.tile is rewritten by the next ticket
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -437,6 +453,64 @@ __global__ void __launch_bounds__(WAVE_THREADS) k_dilu_wave(WaveArgs a) {
       __threadfence();
       atomicAdd(&a.ctl->epoch, 1u);
     }
+  }
+}
+
+// Coefficient streams of the sweeps in the tile-skewed layout, formed once
+// from the factor with the reference's operations (Row7 operand order, FP32
+// division by the pivot); zero where a thread has no point at a step.
+__global__ void k_wave_streams(Geo g, DevMesh m, const float *__restrict__ d, const float *__restrict__ dinv,
+                               int nte, int ntiles, int nsteps, float *__restrict__ lf, float4 *__restrict__ ub) {
+  const long long total = (long long)ntiles * nsteps * WAVE_THREADS;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int T = (int)(q % WAVE_THREADS);
+    const long long r = q / WAVE_THREADS;
+    const int t = (int)(r % nsteps);
+    const int ti = (int)(r / nsteps);
+    const int te = ti % nte, tj = ti / nte;
+    const int el = T & (WE - 1), jl = T / WE;
+    const int e = te * WE + el, jj = tj * WJT + jl;
+    const bool valid = e < g.nrm2 && jj < g.ntm2;
+    float l0 = 0.f, l1 = 0.f, l2 = 0.f;
+    float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int kf = t - (el + jl);
+    if (valid && kf >= 0 && kf < g.npm2) {  // forward point (e, jj, kf)
+      const Row7 c = row7(m, e + 2, jj + 2, kf + 2);
+      if (kf > 0) l0 = __fdiv_rn((float)c.a1, d[g.idx(e, jj, kf - 1)]);
+      if (jj > 0) l1 = __fdiv_rn((float)c.a2, d[g.idx(e, jj - 1, kf)]);
+      if (e > 0) l2 = __fdiv_rn((float)c.a3, d[g.idx(e - 1, jj, kf)]);
+    }
+    const int qb = t - ((WE - 1 - el) + (WJT - 1 - jl));
+    if (valid && qb >= 0 && qb < g.npm2) {  // backward point (e, jj, npm2-1-qb)
+      const int kb = g.npm2 - 1 - qb;
+      const Row7 c = row7(m, e + 2, jj + 2, kb + 2);
+      u.x = e < g.nrm2 - 1 ? (float)c.a5 : 0.f;
+      u.y = jj < g.ntm2 - 1 ? (float)c.a6 : 0.f;
+      u.z = kb < g.npm2 - 1 ? (float)c.a7 : 0.f;
+      u.w = dinv[g.idx(e, jj, kb)];
+    }
+    const size_t base = ((size_t)ti * nsteps + t) * WAVE_THREADS;
+    lf[base * 3 + T] = l0;
+    lf[base * 3 + WAVE_THREADS + T] = l1;
+    lf[base * 3 + 2 * WAVE_THREADS + T] = l2;
+    ub[base + T] = u;
+  }
+}
+
+// Per-line seam coefficients: forward a7/d(e, j, 0) of the last plane,
+// backward a1 of the first plane.
+__global__ void k_wave_seam(Geo g, DevMesh m, const float *__restrict__ d, float *__restrict__ seam_f,
+                            float *__restrict__ seam_b) {
+  const long long n = (long long)g.ntm2 * g.nrm2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(q % g.nrm2), jj = (int)(q / g.nrm2);
+    const long long row = (long long)jj * g.NRP + e;
+    const Row7 cl = row7(m, e + 2, jj + 2, g.npm2 - 1 + 2);
+    seam_f[row] = __fdiv_rn((float)cl.a7, d[g.idx(e, jj, 0)]);
+    const Row7 cf = row7(m, e + 2, jj + 2, 2);
+    seam_b[row] = (float)cf.a1;
   }
 }
 
@@ -459,10 +533,14 @@ struct DiluState {
   std::vector<int> kk_lo, nkk, nblk;  // per level launch shape (factorisation)
   // wavefront sweeps
   unsigned long long *xe = nullptr, *xj = nullptr;
+  float *lf = nullptr, *ys = nullptr;   // forward coefficients, intermediate y (tile-skewed)
+  float4 *ub = nullptr;                  // backward coefficients (tile-skewed)
+  float *seam_f = nullptr, *seam_b = nullptr;
+  int nsteps = 0;
+  size_t wave_smem_f = 0, wave_smem_b = 0;
   int2 *order = nullptr;
   WaveCtl *ctl = nullptr;
   int nte = 0, ntj = 0, ntiles = 0, ndiag = 0, wave_blocks = 0;
-  size_t wave_smem = 0;
 };
 
 static void level_shape(const Geo &g, int l, int *kk_lo, int *nkk, int *nblk) {
@@ -488,7 +566,7 @@ static void launch_factor_level(Solver *s, int l) {
   k_dilu_factor<<<grid, 128, 0, s->stream>>>(a);
 }
 
-// Exchange buffers, tile order and launch shape of the wavefront sweeps.
+// Exchange buffers, streams, tile order and launch shape of the sweeps.
 static int wave_setup(Solver *s) {
   DiluState *D = s->dilu;
   const Geo &g = s->g;
@@ -496,10 +574,16 @@ static int wave_setup(Solver *s) {
   D->ntj = (g.ntm2 + WJT - 1) / WJT;
   D->ntiles = D->nte * D->ntj;
   D->ndiag = g.npm2 + 16;
+  D->nsteps = g.npm2 + WSK;
   const size_t nx = (size_t)D->ntiles * D->ndiag * 16;
+  const size_t ns = (size_t)D->ntiles * D->nsteps * WAVE_THREADS;
   int st;
   if ((st = s->alloc((void **)&D->xe, 8 * nx)) || (st = s->alloc((void **)&D->xj, 8 * nx)) ||
       (st = s->alloc((void **)&D->order, sizeof(int2) * D->ntiles)) ||
+      (st = s->alloc((void **)&D->lf, sizeof(float) * 3 * ns)) || (st = s->alloc((void **)&D->ys, sizeof(float) * ns)) ||
+      (st = s->alloc((void **)&D->ub, sizeof(float4) * ns)) ||
+      (st = s->alloc((void **)&D->seam_f, sizeof(float) * (size_t)g.ntm2 * g.NRP)) ||
+      (st = s->alloc((void **)&D->seam_b, sizeof(float) * (size_t)g.ntm2 * g.NRP)) ||
       (st = s->alloc((void **)&D->ctl, sizeof(WaveCtl))))
     return st;
   // Tickets in order of the tile's first wavefront step WE te + WJT tj
@@ -516,19 +600,19 @@ static int wave_setup(Solver *s) {
   CK(cudaMemcpyAsync(D->order, ord.data(), sizeof(int2) * D->ntiles, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemsetAsync(D->xe, 0, 8 * nx, s->stream));
   CK(cudaMemsetAsync(D->xj, 0, 8 * nx, s->stream));
+  CK(cudaMemsetAsync(D->seam_f, 0, sizeof(float) * (size_t)g.ntm2 * g.NRP, s->stream));
+  CK(cudaMemsetAsync(D->seam_b, 0, sizeof(float) * (size_t)g.ntm2 * g.NRP, s->stream));
   const WaveCtl c0{0u, 0u, 1u, 0};  // tag 0 is the zeroed buffers': sweeps start at 1
   CK(cudaMemcpyAsync(D->ctl, &c0, sizeof(WaveCtl), cudaMemcpyHostToDevice, s->stream));
-  D->wave_smem = sizeof(double) * 2 * (g.np + 1);
-  const size_t smem_total = D->wave_smem + sizeof(WaveSmem);
-  if (smem_total > 48 * 1024) {
-    CK(cudaFuncSetAttribute(k_dilu_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem));
-    CK(cudaFuncSetAttribute(k_dilu_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem));
-  }
+  D->wave_smem_f = sizeof(WaveSmemF);
+  D->wave_smem_b = sizeof(WaveSmemB);
+  CK(cudaFuncSetAttribute(k_dilu_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_f));
+  CK(cudaFuncSetAttribute(k_dilu_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_b));
   int dev = 0, nsm = 0, occ_f = 0, occ_b = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_THREADS, D->wave_smem));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_THREADS, D->wave_smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_THREADS, D->wave_smem_f));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_THREADS, D->wave_smem_b));
   D->wave_blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, D->ntiles));
   return POT3D_OK;
 }
@@ -537,11 +621,13 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   DiluState *D = s->dilu;
   WaveArgs a{};
   a.g = s->g;
-  a.m = s->m;
-  a.in = fwd ? D->r32 : D->y32;
-  a.out = fwd ? D->y32 : D->z32;
-  a.d = fwd ? D->d : D->dinv;
-  a.dfac = D->d;
+  a.r32 = D->r32;
+  a.z32 = D->z32;
+  a.ys = D->ys;
+  a.lf = D->lf;
+  a.ub = D->ub;
+  a.seam_f = D->seam_f;
+  a.seam_b = D->seam_b;
   a.xe = D->xe;
   a.xj = D->xj;
   a.order = D->order;
@@ -552,10 +638,11 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   a.ntj = D->ntj;
   a.ntiles = D->ntiles;
   a.ndiag = D->ndiag;
+  a.nsteps = D->nsteps;
   if (fwd)
-    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS, D->wave_smem, s->stream>>>(a);
+    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS, D->wave_smem_f, s->stream>>>(a);
   else
-    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS, D->wave_smem, s->stream>>>(a);
+    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS, D->wave_smem_b, s->stream>>>(a);
 }
 
 int dilu_setup(Solver *s) {
@@ -593,7 +680,9 @@ int dilu_setup(Solver *s) {
     pot3d_set_error("zero pivot in the ILU(0) factorisation at row " + std::to_string(piv));
     return POT3D_ERR_PIVOT;
   }
-  return POT3D_OK;
+  k_wave_streams<<<148 * 8, NTHR, 0, s->stream>>>(g, s->m, D->d, D->dinv, D->nte, D->ntiles, D->nsteps, D->lf, D->ub);
+  k_wave_seam<<<grid1d((long long)g.ntm2 * g.nrm2), NTHR, 0, s->stream>>>(g, s->m, D->d, D->seam_f, D->seam_b);
+  return pot3d_cuda_status(cudaGetLastError(), "sweep coefficient streams");
 }
 
 void dilu_destroy(Solver *s) {
