@@ -154,8 +154,8 @@ constexpr int WPF = 8;                  // prefetch distance of the streams (ste
 constexpr int WSK = (WE - 1) + (WJT - 1);
 constexpr int WRIN = WSK + 1 + WPF;     // input plane ring (forward r32)
 constexpr int WROUT = 32;               // output plane ring (backward z32), > WSK
+constexpr int WXR = 4;                  // exchange ring depth (chunks)
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
-static_assert(2 * WCH * 16 == WAVE_THREADS, "one exchange word per thread and chunk");
 static_assert(WROUT > WSK, "a plane is flushed after its last line wrote it");
 
 struct WaveCtl {
@@ -209,18 +209,18 @@ struct WaveSmemF {                   // forward sweep
   float lf[WPF][3][WAVE_THREADS];    // coefficient stream, slot = step % WPF
   float rin[WRIN][WAVE_THREADS];     // r32 planes, slot = plane % WRIN
   float y[2][WJT][WE + 1];           // step parity, line values
-  float ring[2][2][WCH][16];         // chunk parity, face (0: e, 1: j), step in chunk, line
+  float ring[WXR][2][WCH][16];       // chunk % WXR, face (0: e, 1: j), step in chunk, line
   int2 tile;
-  int abort;
+  int abort, ready, consumed;
 };
 struct WaveSmemB {                   // backward sweep
   float4 ub[WPF][WAVE_THREADS];      // coefficient stream
   float yin[WPF][WAVE_THREADS];      // y stream
   float zout[WROUT][WAVE_THREADS];   // z32 planes, slot = plane % WROUT
   float y[2][WJT][WE + 1];
-  float ring[2][2][WCH][16];
+  float ring[WXR][2][WCH][16];
   int2 tile;
-  int abort;
+  int abort, ready, consumed;
 };
 
 template <bool FWD>
@@ -234,11 +234,113 @@ struct WaveSmemSel<false> {
   using type = WaveSmemB;
 };
 
+__device__ __forceinline__ void wave_bar_compute() { asm volatile("bar.sync 1, %0;" ::"n"(WAVE_THREADS) : "memory"); }
+// Barrier of the compute warps that also returns whether any of them saw `flag`.
+__device__ __forceinline__ bool wave_bar_compute_any(bool flag) {
+  unsigned r;
+  asm volatile(
+      "{ .reg .pred p, q; setp.ne.u32 p, %1, 0; bar.red.or.pred q, 1, %2, p; selp.u32 %0, 1, 0, q; }"
+      : "=r"(r)
+      : "r"((unsigned)flag), "n"(WAVE_THREADS)
+      : "memory");
+  return r != 0;
+}
+
+// Face geometry of one tile, shared by the compute warps and the exchange warp.
+struct WaveFaces {
+  int te, tj, ti;
+  bool has_in[2];  // a producer tile exists across face 0 (e) / 1 (j)
+  const unsigned long long *src[2];
+};
 template <bool FWD>
-__device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S, unsigned epoch,
-                                          int te, int tj) {
+__device__ __forceinline__ WaveFaces wave_faces(const WaveArgs &a, int te, int tj) {
+  WaveFaces f;
+  f.te = te;
+  f.tj = tj;
+  f.ti = tj * a.nte + te;
+  const int te_in = FWD ? te - 1 : te + 1, tj_in = FWD ? tj - 1 : tj + 1;
+  f.has_in[0] = te_in >= 0 && te_in < a.nte;
+  f.has_in[1] = tj_in >= 0 && tj_in < a.ntj;
+  f.src[0] = a.xe + (size_t)(tj * a.nte + (f.has_in[0] ? te_in : te)) * a.ndiag * 16;
+  f.src[1] = a.xj + (size_t)((f.has_in[1] ? tj_in : tj) * a.nte + te) * a.ndiag * 16;
+  return f;
+}
+// Whether the consumer line `line` of face `face` needs the word of step t.
+template <bool FWD>
+__device__ __forceinline__ bool wave_needed(const WaveArgs &a, const WaveFaces &f, int face, int line, int t) {
+  if (!f.has_in[face]) return false;
+  const int el_c = face == 0 ? (FWD ? 0 : WE - 1) : line, jl_c = face == 0 ? line : (FWD ? 0 : WJT - 1);
+  if (f.te * WE + el_c >= a.g.nrm2 || f.tj * WJT + jl_c >= a.g.ntm2) return false;
+  const int sk_c = FWD ? el_c + jl_c : (WE - 1 - el_c) + (WJT - 1 - jl_c);
+  const int q = t - sk_c;
+  return t < a.ndiag && q >= 0 && q < a.g.npm2;
+}
+__device__ __forceinline__ bool wave_spin(const unsigned long long *p, unsigned epoch, unsigned long long *w) {
+  unsigned it = 0;
+  while ((unsigned)(*w >> 32) != epoch) {
+    if (++it > WAVE_SPIN_LIMIT) return false;
+    if (it > 8) __nanosleep(32);
+    *w = wave_load(p);
+  }
+  return true;
+}
+
+// Exchange warp: fills the face ring WXR chunks ahead of the compute warps.
+// Lane L serves face L >> 4, line L & 15, all WCH steps of a chunk.
+template <bool FWD>
+__device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S,
+                                              const WaveFaces &f, unsigned epoch, int nch) {
+  const int lane = threadIdx.x & 31;
+  const int face = lane >> 4, line = lane & 15;
+  const unsigned long long *src = f.src[face] + line;
+  for (int c = 0; c < nch; c++) {
+    // wait for a free ring slot (the compute warps consumed chunk c - WXR)
+    unsigned it = 0;
+    while (c - *(volatile int *)&S.consumed >= WXR && !*(volatile int *)&S.abort) {
+      if (++it > WAVE_SPIN_LIMIT) {
+        S.abort = 1;
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (*(volatile int *)&S.abort) return;
+    bool ok = true;
+    unsigned long long w[WCH];
+    // the chunk's last needed word of this line first: once it is current
+    // the earlier ones (published earlier by the same producer thread) are
+    // almost always visible too
+    int last = -1;
+#pragma unroll
+    for (int s = 0; s < WCH; s++)
+      if (wave_needed<FWD>(a, f, face, line, c * WCH + s)) last = s;
+    if (last >= 0) {
+      unsigned long long wl = wave_load(src + (size_t)(c * WCH + last) * 16);
+      ok = wave_spin(src + (size_t)(c * WCH + last) * 16, epoch, &wl);
+#pragma unroll
+      for (int s = 0; s < WCH; s++)
+        w[s] = (s <= last && wave_needed<FWD>(a, f, face, line, c * WCH + s)) ? wave_load(src + (size_t)(c * WCH + s) * 16)
+                                                                                : ((unsigned long long)epoch << 32);
+#pragma unroll
+      for (int s = 0; s < WCH; s++) {
+        ok = ok && wave_spin(src + (size_t)(c * WCH + s) * 16, epoch, &w[s]);
+        S.ring[c % WXR][face][s][line] = __uint_as_float((unsigned)w[s]);
+      }
+    }
+    if (!ok) S.abort = 1;
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      *(volatile int *)&S.ready = c + 1;
+    }
+  }
+}
+
+template <bool FWD>
+__device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S, const WaveFaces &f,
+                                          unsigned epoch) {
   const Geo &g = a.g;
   const int T = threadIdx.x;
+  const int te = f.te, tj = f.tj, ti = f.ti;
   const int el = T & (WE - 1), jl = T / WE;
   const int e = te * WE + el, jj = tj * WJT + jl;
   const bool valid = e < g.nrm2 && jj < g.ntm2;
@@ -246,89 +348,44 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
   const int npm2 = g.npm2;
   const long long plane = (long long)g.ntm2 * g.NRP;
   const long long row = (long long)(valid ? jj : 0) * g.NRP + (valid ? e : 0);
-  const int ti = tj * a.nte + te;
   const size_t tbase = (size_t)ti * a.nsteps * WAVE_THREADS;  // tile-skewed stream base
-  // neighbour tiles across the faces this tile consumes and produces
-  const int te_in = FWD ? te - 1 : te + 1, tj_in = FWD ? tj - 1 : tj + 1;
   const int te_out = FWD ? te + 1 : te - 1, tj_out = FWD ? tj + 1 : tj - 1;
-  const bool has_in_e = te_in >= 0 && te_in < a.nte, has_in_j = tj_in >= 0 && tj_in < a.ntj;
   const bool pub_e = valid && (FWD ? el == WE - 1 : el == 0) && te_out >= 0 && te_out < a.nte;
   const bool pub_j = valid && (FWD ? jl == WJT - 1 : jl == 0) && tj_out >= 0 && tj_out < a.ntj;
   const bool ext_e = FWD ? el == 0 : el == WE - 1;    // e-neighbour across the face
   const bool ext_j = FWD ? jl == 0 : jl == WJT - 1;   // j-neighbour across the face
   const bool cpl_e = valid && (FWD ? e > 0 : e < g.nrm2 - 1);
   const bool cpl_j = valid && (FWD ? jj > 0 : jj < g.ntm2 - 1);
-  unsigned long long *xe_out = a.xe + (size_t)ti * a.ndiag * 16;
-  unsigned long long *xj_out = a.xj + (size_t)ti * a.ndiag * 16;
+  unsigned long long *xe_out = a.xe + (size_t)ti * a.ndiag * 16 + jl - (size_t)(WE - 1) * 16;
+  unsigned long long *xj_out = a.xj + (size_t)ti * a.ndiag * 16 + el - (size_t)(WJT - 1) * 16;
   const float seam_c = valid ? (FWD ? a.seam_f[row] : a.seam_b[row]) : 0.f;
-  // exchange slot of this thread: face xf, step xs of the chunk, line xl
-  const int xf = T >> 7, xs = (T >> 4) & (WCH - 1), xl = T & 15;
-  const bool x_tile = xf == 0 ? has_in_e : has_in_j;
-  const unsigned long long *x_src =
-      xf == 0 ? a.xe + (size_t)(tj * a.nte + (x_tile ? te_in : te)) * a.ndiag * 16
-              : a.xj + (size_t)((x_tile ? tj_in : tj) * a.nte + te) * a.ndiag * 16;
-  // the consumer of slot (xf, *, xl): thread (el_c, jl_c) of this tile
-  const int el_c = xf == 0 ? (FWD ? 0 : WE - 1) : xl, jl_c = xf == 0 ? xl : (FWD ? 0 : WJT - 1);
-  const int sk_c = FWD ? el_c + jl_c : (WE - 1 - el_c) + (WJT - 1 - jl_c);
-  const bool x_line = x_tile && te * WE + el_c < g.nrm2 && tj * WJT + jl_c < g.ntm2;
-  auto x_needed = [&](int t) {
-    const int q = t - sk_c;
-    return x_line && t < a.ndiag && q >= 0 && q < npm2;
-  };
-  unsigned long long xw = 0;  // word of the next chunk
-  auto x_fetch = [&](int c) {
-    const int t = c * WCH + xs;
-    if (x_needed(t)) xw = wave_load(x_src + (size_t)t * 16 + xl);
-  };
-  // Poll one word until its tag is current (bounded); false on a timeout.
-  auto x_poll = [&](int t, unsigned long long *w) {
-    unsigned it = 0;
-    while ((unsigned)(*w >> 32) != epoch) {
-      if (++it > WAVE_SPIN_LIMIT) return false;
-      if (it > 4) __nanosleep(it < 64 ? 32 : 256);
-      *w = wave_load(x_src + (size_t)t * 16 + xl);
-    }
-    return true;
-  };
-  // One thread per face waits for the chunk's last word of line 0: all
-  // lines of one step are published at the same producer step, so after it
-  // the chunk's other words are (almost always) visible too.
-  auto x_lead = [&](int c) {
-    const int t = c * WCH + xs;
-    if (xs == WCH - 1 && xl == 0 && x_needed(t)) return x_poll(t, &xw);
-    return true;
-  };
-  // Commit the fetched chunk c into ring slot c & 1; false on a timeout.
-  auto x_commit = [&](int c) {
-    const int t = c * WCH + xs;
-    bool ok = true;
-    if (x_needed(t)) {
-      if ((unsigned)(xw >> 32) != epoch) xw = wave_load(x_src + (size_t)t * 16 + xl);
-      ok = x_poll(t, &xw);
-      S.ring[c & 1][xf][xs][xl] = __uint_as_float((unsigned)xw);
-    }
-    return ok;
-  };
-
-  auto kk_of = [&](int t) { return FWD ? t - sk : npm2 - 1 - (t - sk); };
-  auto active = [&](int t) { return valid && t - sk >= 0 && t - sk < npm2; };
   const int nsteps = a.nsteps;
+  const int nch = (nsteps + WCH - 1) / WCH;
+  // ring entries this thread reads for its out-of-tile neighbours
+  const int ring_e = (0 * WCH) * 16 + jl, ring_j = (1 * WCH) * 16 + el;
+  const int y_e = ext_e ? 0 : jl * (WE + 1) + (FWD ? el - 1 : el + 1);
+  const int y_j = ext_j ? 0 : (FWD ? jl - 1 : jl + 1) * (WE + 1) + el;
+
   // Streams: one copy group per step, issued WPF steps before it is read.
   // Forward: the coefficients of step t+WPF and this line's r32 of plane
   // t+WPF (read at the step t+WPF+s that handles it).  Backward: the
   // coefficients and y of step t+WPF (y in reversed forward step order).
+  const float *lf_p = a.lf + tbase * 3 + T;
+  const float4 *ub_p = a.ub + tbase + T;
+  const float *ys_p = a.ys + tbase + T;
+  const float *r_p = a.r32 + row;
   auto issue = [&](int t) {
     const bool in_t = t < nsteps;
-    const size_t so = tbase + (size_t)(in_t ? t : 0) * WAVE_THREADS + T;
     if constexpr (FWD) {
-      const size_t lo = tbase * 3 + (size_t)(in_t ? t : 0) * 3 * WAVE_THREADS + T;
-      for (int c3 = 0; c3 < 3; c3++) cp_async4(&S.lf[t & (WPF - 1)][c3][T], a.lf + lo + c3 * WAVE_THREADS, in_t);
+      const float *l = lf_p + (size_t)(in_t ? t : 0) * 3 * WAVE_THREADS;
+      cp_async4(&S.lf[t & (WPF - 1)][0][T], l, in_t);
+      cp_async4(&S.lf[t & (WPF - 1)][1][T], l + WAVE_THREADS, in_t);
+      cp_async4(&S.lf[t & (WPF - 1)][2][T], l + 2 * WAVE_THREADS, in_t);
       const bool rp = valid && t < npm2;
-      cp_async4(&S.rin[t % WRIN][T], a.r32 + row + (rp ? (long long)t * plane : 0), rp);
+      cp_async4(&S.rin[t % WRIN][T], r_p + (rp ? (long long)t * plane : 0), rp);
     } else {
-      cp_async16(&S.ub[t & (WPF - 1)][T], a.ub + so, in_t);
-      const size_t yo = tbase + (size_t)(in_t ? nsteps - 1 - t : 0) * WAVE_THREADS + T;
-      cp_async4(&S.yin[t & (WPF - 1)][T], a.ys + yo, in_t);
+      cp_async16(&S.ub[t & (WPF - 1)][T], ub_p + (size_t)(in_t ? t : 0) * WAVE_THREADS, in_t);
+      cp_async4(&S.yin[t & (WPF - 1)][T], ys_p + (size_t)(in_t ? nsteps - 1 - t : 0) * WAVE_THREADS, in_t);
     }
     cp_async_commit();
   };
@@ -336,25 +393,29 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
   for (int t = 0; t < WPF; t++) issue(t);
   float seam_y = 0.f;  // value at the line's first plane of the sweep
   float prev = 0.f;    // own value at the previous step
-  const int nch = (nsteps + WCH - 1) / WCH;
-  bool ok = true;
-  x_fetch(0);
+  int rslot = (WRIN - (sk % WRIN)) % WRIN;  // (t - sk) mod WRIN at t = 0
 #pragma unroll 1
   for (int c = 0; c < nch; c++) {
-    if (!x_lead(c)) S.abort = 1;
-    __syncthreads();
-    ok = x_commit(c);
-    x_fetch(c + 1);
-    if (!ok) S.abort = 1;
-    __syncthreads();
-    if (S.abort) {
+    {  // wait until the exchange warp has chunk c in the ring
+      unsigned it = 0;
+      while (*(volatile int *)&S.ready <= c && !*(volatile int *)&S.abort) {
+        if (++it > WAVE_SPIN_LIMIT) {
+          S.abort = 1;
+          break;
+        }
+        if (it > 4) __nanosleep(32);
+      }
+      __threadfence_block();
+    }
+    if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) {  // uniform over the compute warps
       cp_async_wait<0>();
       return false;
     }
+    const float *ring = &S.ring[c % WXR][0][0][0];
 #pragma unroll
     for (int u = 0; u < WCH; u++) {
       const int t = c * WCH + u;
-      const int p = (t + 1) & 1;  // buffer of step t-1
+      const float *yprev = &S.y[(t + 1) & 1][0][0];  // values of step t-1
       if constexpr (!FWD) {
         // flush the z32 plane whose last line was written at step t-1
         const int kd = npm2 + WSK - t;
@@ -363,24 +424,25 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
       cp_async_wait<WPF - 1>();  // this step's group (and every older one) has landed
       float v_in, c0, c1, c2, c3 = 0.f;
       if constexpr (FWD) {
-        c0 = S.lf[t & (WPF - 1)][0][T];
-        c1 = S.lf[t & (WPF - 1)][1][T];
-        c2 = S.lf[t & (WPF - 1)][2][T];
-        const int kr = t - sk;
-        v_in = S.rin[(kr >= 0 ? kr : 0) % WRIN][T];
+        c0 = S.lf[u & (WPF - 1)][0][T];
+        c1 = S.lf[u & (WPF - 1)][1][T];
+        c2 = S.lf[u & (WPF - 1)][2][T];
+        v_in = S.rin[rslot][T];
       } else {
-        const float4 cf = S.ub[t & (WPF - 1)][T];
+        const float4 cf = S.ub[u & (WPF - 1)][T];
         c0 = cf.x;
         c1 = cf.y;
         c2 = cf.z;
         c3 = cf.w;
-        v_in = S.yin[t & (WPF - 1)][T];
+        v_in = S.yin[u & (WPF - 1)][T];
       }
+      rslot = rslot + 1 == WRIN ? 0 : rslot + 1;
       issue(t + WPF);
-      if (active(t)) {
-        const int kk = kk_of(t);
-        const float ne = ext_e ? S.ring[c & 1][0][u][jl] : S.y[p][jl][FWD ? el - 1 : el + 1];
-        const float nj = ext_j ? S.ring[c & 1][1][u][el] : S.y[p][FWD ? jl - 1 : jl + 1][el];
+      const int q = t - sk;
+      if (valid && (unsigned)q < (unsigned)npm2) {
+        const int kk = FWD ? q : npm2 - 1 - q;
+        const float ne = ext_e ? ring[ring_e + u * 16] : yprev[y_e];
+        const float nj = ext_j ? ring[ring_j + u * 16] : yprev[y_j];
         float y = v_in;
         if (FWD) {
           // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1)
@@ -403,12 +465,13 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
           a.ys[tbase + (size_t)t * WAVE_THREADS + T] = y;
         else
           S.zout[kk % WROUT][T] = y;
-        if (pub_e) wave_publish(xe_out + (size_t)(t - (WE - 1)) * 16 + jl, epoch, y);
-        if (pub_j) wave_publish(xj_out + (size_t)(t - (WJT - 1)) * 16 + el, epoch, y);
+        if (pub_e) wave_publish(xe_out + (size_t)t * 16, epoch, y);
+        if (pub_j) wave_publish(xj_out + (size_t)t * 16, epoch, y);
         prev = y;
       }
-      __syncthreads();
+      wave_bar_compute();
     }
+    if (T == 0) *(volatile int *)&S.consumed = c + 1;
   }
   if constexpr (!FWD) {  // the first plane completes at the last step
     const int kd = npm2 + WSK - nsteps;
@@ -419,30 +482,39 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
 }
 
 template <bool FWD>
-__global__ void __launch_bounds__(WAVE_THREADS, 3) k_dilu_wave(WaveArgs a) {
+__global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) {
   using Sm = typename WaveSmemSel<FWD>::type;
   extern __shared__ float4 wave_dyn[];
   Sm &S = *reinterpret_cast<Sm *>(wave_dyn);
-  if (threadIdx.x == 0) S.abort = 0;
-  __syncthreads();
+  const bool xwarp = threadIdx.x >= WAVE_THREADS;
   const unsigned epoch = *(volatile unsigned *)&a.ctl->epoch;
   const bool run = !(a.check && *(volatile int *)&a.st->status != ST_RUNNING);
   while (run) {
     if (threadIdx.x == 0) {
       const unsigned t = atomicAdd(&a.ctl->ticket, 1u);
       S.tile = t < (unsigned)a.ntiles ? a.order[FWD ? t : a.ntiles - 1 - t] : make_int2(-1, -1);
+      S.abort = 0;
+      S.ready = 0;
+      S.consumed = 0;
     }
     __syncthreads();
     const int2 tile = S.tile;
     if (tile.x < 0) break;
-    if (!wave_tile<FWD>(a, S, epoch, tile.x, tile.y)) {
+    const WaveFaces f = wave_faces<FWD>(a, tile.x, tile.y);
+    bool ok = true;
+    if (xwarp)
+      wave_exchange<FWD>(a, S, f, epoch, (a.nsteps + WCH - 1) / WCH);
+    else
+      ok = wave_tile<FWD>(a, S, f, epoch);
+    if (!ok) S.abort = 1;
+    __syncthreads();
+    if (S.abort) {
       if (threadIdx.x == 0) {
         atomicExch(&a.ctl->error, 1);
         if (a.st) atomicExch(&a.st->status, ST_TIMEOUT);
       }
       break;
     }
-    __syncthreads();  // S.tile is rewritten by the next ticket
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -611,8 +683,8 @@ static int wave_setup(Solver *s) {
   int dev = 0, nsm = 0, occ_f = 0, occ_b = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_THREADS, D->wave_smem_f));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_THREADS, D->wave_smem_b));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_THREADS + 32, D->wave_smem_f));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_THREADS + 32, D->wave_smem_b));
   D->wave_blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, D->ntiles));
   return POT3D_OK;
 }
@@ -640,9 +712,9 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   a.ndiag = D->ndiag;
   a.nsteps = D->nsteps;
   if (fwd)
-    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS, D->wave_smem_f, s->stream>>>(a);
+    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_f, s->stream>>>(a);
   else
-    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS, D->wave_smem_b, s->stream>>>(a);
+    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_b, s->stream>>>(a);
 }
 
 int dilu_setup(Solver *s) {
