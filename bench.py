@@ -3,17 +3,23 @@
 One step = one complete PCG solve of the PFSS workload 255x361x721 (65.3 M
 unknowns, seeded synthetic Br: spherical harmonics l<=40 plus 20 bipoles),
 from a zero guess to the reference's stopping rule epsn < epscg = 1e-9
-(ernorm, src/pot3d.F90:4430-4433).
+(ernorm, src/pot3d.F90:4430-4433).  The default solver is the reference's
+ILU(0) preconditioner (ifprec=2) applied in FP32 by the wavefront sweeps
+inside FP64 PCG; the plain FP64 PCG with the diagonal preconditioner
+(ifprec=1, the reference's default) is timed in the same run and reported
+beside it (`plain_fp64`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload NAME] [--ifprec 1|2] [--precision fp64|fp32_refined]
+                    [--no-plain]
 
 value: device time of the solve (CUDA events on the library's stream around
 the PCG initialisation and iterations), inputs resident in HBM.
 e2e: the same solve through the C-ABI with host buffers, pot3d_gpu_cgsolve,
 host<->device copies of x and r included, wall time.
-The working set (~2.6 GB of vectors) is 20x the 126 MB L2, so no flush is
-needed between steps.
+The working set (~2.6 GB of vectors, plus ~2.5 GB of sweep coefficient
+streams with ILU(0)) is 20x the 126 MB L2, so no flush is needed between
+steps.
 
 Multi-GPU: replicas only (each rank solves its own instance); the reported
 time is the maximum over ranks.
@@ -34,6 +40,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "solve s to 1e-9 resid: learned+FP32-refined vs plain FP64 PCG on 1 B200; HBM GB/s"
+# Iteration counts of the seeded workloads' GPU solves (FP64 PCG to 1e-9),
+# used to project the reference arm's CPU sample to a whole solve.
+SOLVE_ITERATIONS = {("pfss_255x361x721", 1): 7036, ("pfss_255x361x721", 2): 1094}
+# Algorithmic DRAM bytes per unknown and PCG iteration: diagonal
+# preconditioner 80 (stencil r, p -> p, Ap; update x, p, r, Ap -> x, r);
+# ILU(0) 136 (stencil p, z32 -> p, Ap: 28; update x, p, r, Ap -> x, r, r32:
+# 52; forward sweep r32, 3 coefficients -> y: 20; backward sweep y, 3
+# coefficients + dinv -> z32: 24; r.z: 12).
+BYTES_PER_UNKNOWN_ITER = {1: 80.0, 2: 136.0}
+SWEEP_BYTES_PER_UNKNOWN = {"k_dilu_wave<fwd>": 20.0, "k_dilu_wave<bwd>": 24.0}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -196,7 +212,7 @@ def run_reference(args):
     # iterations as the FP64 GPU path; the count of the seeded workload at
     # this size is recorded once per run by a short GPU-free estimate: the
     # projection uses the iteration count of the FP64 solve of this workload.
-    ncg = args.ref_iterations
+    ncg = args.ref_iterations or SOLVE_ITERATIONS.get((args.workload, args.ifprec), 6500)
     vals = []
     for _ in range(args.warmup + args.steps):
         cb = cpu_baseline(mesh, br0, opt, args.ifprec, ncg, args.cpu_sample_iters)
@@ -219,20 +235,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pfss_255x361x721")
-    ap.add_argument("--ifprec", type=int, default=1)
+    ap.add_argument("--ifprec", type=int, default=2)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"])
     ap.add_argument("--epscg", type=float, default=1e-9)
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="iteration count used to project the CPU sample (0: take it from a GPU solve)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain FP64 PCG (ifprec=1) solve timed beside the headline solve")
     ap.add_argument("--kernel-timing-only", action="store_true",
                     help="time the stencil and update kernels once (used for ncu captures) and exit")
     args = ap.parse_args()
 
     if args.impl == "reference":
-        if args.ref_iterations <= 0:
-            args.ref_iterations = 6500
         return run_reference(args)
 
     ws, rank, local = dist_init()
@@ -297,13 +313,37 @@ def main():
         ms, by = s.time_kernels(20)
         kern = {"k_stencil": {"ms": ms[0], "bytes": by[0], "gbs": by[0] / (ms[0] * 1e-3) / 1e9},
                 "k_update": {"ms": ms[1], "bytes": by[1], "gbs": by[1] / (ms[1] * 1e-3) / 1e9}}
+    elif args.ifprec == 2:
+        fms, bms = s.time_sweeps(10)
+        kern = {}
+        for name, t in (("k_dilu_wave<fwd>", fms), ("k_dilu_wave<bwd>", bms)):
+            by = SWEEP_BYTES_PER_UNKNOWN[name] * N
+            kern[name] = {"ms": t, "bytes": by, "gbs": by / (t * 1e-3) / 1e9}
+
+    # The plain FP64 PCG (diagonal preconditioner) on the same inputs.
+    plain = None
+    if args.ifprec == 2 and not args.no_plain:
+        sp = Pot3dSolver(mesh, br0, option=opt, ifprec=1, precision="fp64", device=local)
+        pt = []
+        for it in range(2):
+            xt.zero_()
+            rt.copy_(bt)
+            torch.cuda.synchronize()
+            if sp.cgsolve_dev(xt, rt, epscg=args.epscg) != 0:
+                raise SystemExit("plain FP64 solve did not converge")
+            pt.append(sp.last_info.seconds)
+        p_ncg = sp.last_info.ncg
+        sp.close()
+        t_plain = reduce_max(pt[-1], ws)
+        plain = {"seconds": t_plain, "iterations": p_ncg, "ifprec": 1, "precision": "fp64",
+                 "speedup": t_plain / t_dev}
 
     if rank != 0:
         s.close()
         return 0
     peak, psrc = peak_hbm()
     ncg = int(np.median(ncgs))
-    bytes_per_iter = (80.0 if args.ifprec != 2 else 104.0) * N
+    bytes_per_iter = BYTES_PER_UNKNOWN_ITER[2 if args.ifprec == 2 else 1] * N
     overall_gbs = bytes_per_iter * ncg / t_dev / 1e9
     roofline = None
     if kern:
@@ -327,7 +367,7 @@ def main():
                    "l2": "working set ~2.6 GB >> 126 MB L2, no flush"},
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 16 * N},
         "roofline": roofline, "cpu_baseline": cb, "clocks": clk.summary(),
-        "gpu_launches": launches, "true_residual": tres, "epsn": epsn,
+        "gpu_launches": launches, "true_residual": tres, "epsn": epsn, "plain_fp64": plain,
         "throughput_solves_per_s": ws / t_dev,
     }
     print(json.dumps(line), flush=True)
