@@ -61,15 +61,16 @@ def peak_hbm():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def measured_traffic(kernel: str):
-    """Per-launch DRAM bytes of a kernel from the committed ncu summary
-    (profiles/ncu_traffic.txt: 'kernel workload bytes_per_launch'), or None."""
+def measured_traffic(kernel: str, workload: str):
+    """Per-launch DRAM bytes of a kernel on a workload from the committed ncu
+    summary (profiles/ncu_traffic.txt: 'kernel workload bytes_per_launch'),
+    or None."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(p):
         return None
     for ln in open(p):
         f = ln.split()
-        if len(f) >= 3 and f[0] == kernel and not ln.startswith("#"):
+        if len(f) >= 3 and f[0] == kernel and f[1] == workload and not ln.startswith("#"):
             try:
                 return float(f[2])
             except ValueError:
@@ -245,7 +246,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain FP64 PCG (ifprec=1) solve timed beside the headline solve")
     ap.add_argument("--kernel-timing-only", action="store_true",
-                    help="time the stencil and update kernels once (used for ncu captures) and exit")
+                    help="time the hot kernels briefly (stencil and update, or with --ifprec 2 the two "
+                         "ILU(0) sweeps; used for ncu captures) and exit")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -259,8 +261,16 @@ def main():
     mesh, br0, opt, seed = build_case(args.workload, rank)
     s = Pot3dSolver(mesh, br0, option=opt, ifprec=args.ifprec, precision=args.precision, device=local)
     if args.kernel_timing_only:
-        ms, by = s.time_kernels(4)
-        print(json.dumps({"workload": args.workload, "ms": list(ms), "gbs": list(by / (ms * 1e-3) / 1e9)}))
+        if args.ifprec == 2:
+            fms, bms = s.time_sweeps(2)
+            out = {}
+            for name, t in (("k_dilu_wave<fwd>", fms), ("k_dilu_wave<bwd>", bms)):
+                by = SWEEP_BYTES_PER_UNKNOWN[name] * s.N
+                out[name] = {"ms": t, "gbs": by / (t * 1e-3) / 1e9}
+            print(json.dumps({"workload": args.workload, "kernels": out}))
+        else:
+            ms, by = s.time_kernels(4)
+            print(json.dumps({"workload": args.workload, "ms": list(ms), "gbs": list(by / (ms * 1e-3) / 1e9)}))
         s.close()
         return 0
     b = s.rhs()
@@ -348,7 +358,7 @@ def main():
     roofline = None
     if kern:
         dom = max(kern, key=lambda k: kern[k]["ms"])
-        tr = measured_traffic(dom)
+        tr = measured_traffic(dom, args.workload)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
                     "frac": kern[dom]["gbs"] / peak, "traffic": tr, "peak_source": f"{psrc} (MEASURED_PEAKS.json hbm_gbs)"
                     if psrc == "measured" else psrc,
