@@ -343,6 +343,40 @@ class FNO:
                                            C.c_void_p(wb.data_ptr()) if wb is not None else None, w.numel(), lr, b1,
                                            b2, eps, self.step_count, _stream()))
 
+    # ----------------------------------------------------------- weights
+    def save(self, path):
+        """Parameters as BF16 bits (matrices, the precision inference uses)
+        and FP32 (bias vectors), with the grid they were trained on."""
+        import torch
+        out = {"grid": np.array([self.g.nth, self.g.nph, self.g.R, self.W, self.nl, self.mt, self.mp, self.hidden,
+                                 self.in_ch], np.int64)}
+        for k, v in self.p.items():
+            if v.dim() >= 2:
+                out["bf16_" + k] = v.to(torch.bfloat16).view(torch.int16).cpu().numpy()
+            else:
+                out["f32_" + k] = v.cpu().numpy()
+        np.savez_compressed(path, **out)
+
+    @classmethod
+    def load(cls, path, grid: "Grid"):
+        """A model saved by save() for the same grid (theta, phi, radial sizes)."""
+        import torch
+        z = np.load(path)
+        nth, nph, R, W_, nl, mt, mp, hidden, in_ch = (int(v) for v in z["grid"])
+        if (nth, nph, R) != (grid.nth, grid.nph, grid.R):
+            raise ValueError(f"{path}: trained for {nth}x{nph}x{R}, not {grid.nth}x{grid.nph}x{grid.R}")
+        m = cls(grid, width=W_, layers=nl, mt=mt, mp=mp, hidden=hidden, in_ch=in_ch)
+        for k in list(m.p):
+            if "bf16_" + k in z:
+                t = torch.from_numpy(z["bf16_" + k]).view(torch.bfloat16).to(torch.float32)
+            else:
+                t = torch.from_numpy(z["f32_" + k])
+            if tuple(t.shape) != tuple(m.p[k].shape):
+                raise ValueError(f"{path}: parameter {k} has shape {tuple(t.shape)}")
+            m.p[k].copy_(t.cuda())
+        m.pb = {k: v.to(torch.bfloat16).contiguous() for k, v in m.p.items() if v.dim() >= 2}
+        return m
+
     def predict(self, x, sigma):
         """Initial guesses in the packed solver layout, FP64 [B, N]."""
         import torch

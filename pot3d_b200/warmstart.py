@@ -2,7 +2,8 @@
 held-out evaluation of PCG from the predicted guess against PCG from zero.
 
     python -m pot3d_b200.warmstart --nr 127 --nt 181 --np 361 \\
-        --train 2000 --test 200 --epochs 20 --out results.json
+        --train 2000 --test 200 --epochs 20 --out results.json [--save model.npz]
+        [--ifprec 2] [--no-refined]
 
 Training pairs are (Br0 map, phi) of seeded synthetic PFSS cases solved by
 the FP64 GPU PCG (`--train-eps`, default 1e-7: the network is far less
@@ -239,10 +240,12 @@ def main(argv=None):
     ap.add_argument("--out", default="warmstart.json")
     ap.add_argument("--save", default="")
     ap.add_argument("--no-augment", action="store_true")
+    ap.add_argument("--ifprec", type=int, default=1, help="preconditioner of the generating and evaluating solves")
+    ap.add_argument("--no-refined", action="store_true", help="skip the FP32-refined evaluation solves")
     args = ap.parse_args(argv)
     import torch
     mesh = host.make_mesh(args.nr, args.nt, args.np)
-    solver = Pot3dSolver(mesh, case_br0(mesh, args.train_seed0, args.lmax, args.nbip))
+    solver = Pot3dSolver(mesh, case_br0(mesh, args.train_seed0, args.lmax, args.nbip), ifprec=args.ifprec)
     model = FNO(grid_from_mesh(mesh))
     inputs = Inputs(model)
     t0 = time.time()
@@ -259,7 +262,8 @@ def main(argv=None):
     from .tc import check_errors
     check_errors()
     del br0n, tgt
-    solver32 = Pot3dSolver(mesh, case_br0(mesh, args.test_seed0, args.lmax, args.nbip), precision="fp32_refined")
+    solver32 = None if args.no_refined else Pot3dSolver(mesh, case_br0(mesh, args.test_seed0, args.lmax, args.nbip),
+                                                        precision="fp32_refined")
     summ, rows = evaluate(model, inputs, mesh, solver, range(args.test_seed0, args.test_seed0 + args.test),
                           args.lmax, args.nbip, solver32=solver32)
     t3 = time.time()
@@ -269,7 +273,7 @@ def main(argv=None):
         json.dump(rep, fh, indent=1)
     print(json.dumps(summ), flush=True)
     if args.save:
-        torch.save({k: v.cpu() for k, v in model.p.items()}, args.save)
+        model.save(args.save)
     return 0
 
 

@@ -64,3 +64,23 @@ def test_fno_inference_equals_training_forward(cuda):
     b = model.forward(x, keep=False)
     torch.cuda.synchronize()
     assert torch.equal(a, b)
+
+
+def test_fno_save_load_roundtrip(cuda, tmp_path):
+    """A saved operator reloads with the BF16 weights inference uses and
+    predicts the same guess; a model for another grid is rejected."""
+    import torch
+    from pot3d_b200 import host
+    from pot3d_b200.fno import FNO, grid_from_mesh
+    mesh = host.make_mesh(20, 21, 33)
+    g = grid_from_mesh(mesh)
+    m = FNO(g, seed=3)
+    tn, pn, fi = host.synthetic_br(4, 8, 2, 21, 33)
+    x, sig = m.inputs([host.br0_from_map(mesh, tn, pn, fi)])
+    p0 = m.predict(x, sig)
+    path = str(tmp_path / "m.npz")
+    m.save(path)
+    m2 = FNO.load(path, g)
+    assert torch.equal(m2.predict(x, sig), p0)
+    with pytest.raises(ValueError):
+        FNO.load(path, grid_from_mesh(host.make_mesh(20, 21, 35)))
