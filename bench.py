@@ -243,6 +243,9 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="iteration count used to project the CPU sample (0: take it from a GPU solve)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--warm-start", default="auto",
+                    help="FNO weights (.npz) for the learned initial guess; 'auto' uses "
+                         "pot3d_b200/weights/fno_<workload>.npz when present; 'off' solves from zero")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain FP64 PCG (ifprec=1) solve timed beside the headline solve")
     ap.add_argument("--kernel-timing-only", action="store_true",
@@ -279,13 +282,44 @@ def main():
     rt = torch.empty(N, dtype=torch.float64, device="cuda")
     bt = torch.tensor(b, device="cuda")
 
-    def solve_resident():
-        xt.zero_()
+    # Learned initial guess (FNO trained on this grid), inference timed as part of the solve.
+    wpath = args.warm_start
+    if wpath == "auto":
+        cand = os.path.join(ROOT, "pot3d_b200", "weights", f"fno_{args.workload}.npz")
+        wpath = cand if os.path.exists(cand) else "off"
+    model = None
+    if wpath != "off":
+        from pot3d_b200.fno import FNO, grid_from_mesh
+        from pot3d_b200.tc import LAUNCHES, check_errors
+        from pot3d_b200.warmstart import Inputs
+        model = FNO.load(wpath, grid_from_mesh(mesh))
+        inputs = Inputs(model)
+        v, sig = inputs.normalized(br0)
+        br0n_h = torch.from_numpy(v).view(1, -1).pin_memory()
+        br0n_d = br0n_h.cuda()
+        sig_d = torch.tensor([sig], dtype=torch.float64, device="cuda")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def guess_into(x):
+        """Inference into x; returns (seconds, kernel launches)."""
+        n0 = LAUNCHES[0]
+        ev0.record()
+        model.predict(inputs.build(br0n_d), sig_d, out=x.view(1, -1))
+        ev1.record()
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) * 1e-3, LAUNCHES[0] - n0
+
+    def solve_resident(learned=True):
+        t_inf, n_inf = 0.0, 0
+        if model is not None and learned:
+            t_inf, n_inf = guess_into(xt)
+        else:
+            xt.zero_()
         rt.copy_(bt)
         torch.cuda.synchronize()
         ierr = s.cgsolve_dev(xt, rt, epscg=args.epscg)
         inf = s.last_info
-        return ierr, inf.seconds, inf.ncg, inf.epsn, inf.true_resid, inf.kernel_launches, inf.n_refine
+        return ierr, inf.seconds + t_inf, inf.ncg, inf.epsn, inf.true_resid, inf.kernel_launches + n_inf, inf.n_refine
 
     for _ in range(args.warmup):
         solve_resident()
@@ -304,18 +338,35 @@ def main():
     barrier(ws)
     t_dev = reduce_max(float(np.mean(dev_times)), ws)
 
-    # End to end through the host-pointer C-ABI (H2D + solve + D2H).
+    # End to end through the host-pointer C-ABI (H2D + solve + D2H); with the
+    # learned guess also the map's upload and the guess's download.
     x_h = np.zeros(N)
     r_h = np.empty(N)
     e2e = []
+    h2d, d2h = 16 * N, 16 * N
     for it in range(args.steps):
-        x_h[:] = 0.0
         r_h[:] = b
         barrier(ws)
         t0 = time.perf_counter()
+        if model is not None:
+            br0n_d.copy_(br0n_h)
+            guess_into(xt)
+            x_h[:] = xt.cpu().numpy()
+        else:
+            x_h[:] = 0.0
         s.cgsolve(x_h, r_h, epscg=args.epscg)
         e2e.append(time.perf_counter() - t0)
+    if model is not None:
+        h2d += 4 * br0n_h.numel()
+        d2h += 8 * N
+        check_errors()
     t_e2e = reduce_max(float(np.mean(e2e)), ws)
+
+    # The same solver from a zero guess (what the learned guess saves).
+    zero_guess = None
+    if model is not None:
+        ierr0, sec0, ncg0, *_ = solve_resident(learned=False)
+        zero_guess = {"seconds": reduce_max(sec0, ws), "iterations": ncg0}
 
     # Live kernel timing (CUDA events on the library's stream).
     kern = None
@@ -373,11 +424,13 @@ def main():
         "ms_per_step": t_dev * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": args.workload, "unknowns": N, "ifprec": args.ifprec, "precision": args.precision,
+                   "initial_guess": "learned (FNO)" if model is not None else "zero",
                    "epscg": args.epscg, "seed": seed, "iterations": ncg, "parallelism": "replicas",
                    "l2": "working set ~2.6 GB >> 126 MB L2, no flush"},
-        "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 16 * N},
+        "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roofline, "cpu_baseline": cb, "clocks": clk.summary(),
         "gpu_launches": launches, "true_residual": tres, "epsn": epsn, "plain_fp64": plain,
+        "warm_start": None if model is None else {"weights": os.path.relpath(wpath, ROOT), "zero_guess": zero_guess},
         "throughput_solves_per_s": ws / t_dev,
     }
     print(json.dumps(line), flush=True)

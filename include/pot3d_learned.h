@@ -47,6 +47,11 @@ int pot3d_fno_adam(float *w, const float *g, float *m1, float *m2, void *wb, lon
 /* Network inputs x[b][p][64] (BF16): channel 0 = br0n[b][p], channels 1..3 =
  * consts[p][0..2], the rest 0. */
 int pot3d_fno_inputs(const float *br0n, const float *consts, long long B, long long npos, void *x, void *stream);
+/* Initial guesses from the network output: x[b][pos*R + i] = sigma[b] *
+ * out[b][pos][i] for i < R (out FP32 with Rp >= R channels per position,
+ * sigma FP64 on the device, x FP64 in the solver's packed layout). */
+int pot3d_fno_guess(const float *out, long long B, long long npos, int Rp, int R, const double *sigma, double *x,
+                    void *stream);
 
 #ifdef __cplusplus
 }

@@ -274,3 +274,30 @@ extern "C" int pot3d_fno_inputs(const float *br0n, const float *consts, long lon
                                                                      reinterpret_cast<__nv_bfloat16 *>(x));
   return pot3d_cuda_status(cudaGetLastError(), "pot3d_fno_inputs");
 }
+
+namespace {
+// x[b][pos * R + i] = sigma[b] * out[b][pos][i], i < R: the network output
+// (FP32, Rp channels per position) cropped to the radial levels and scaled
+// back to the solver's packed FP64 layout (positions (phi, theta), r fastest).
+__global__ void k_guess(const float *__restrict__ out, long long B, long long npos, int Rp, int R,
+                        const double *__restrict__ sigma, double *__restrict__ x) {
+  const long long n = B * npos * R;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % R);
+    const long long bp = t / R;  // b * npos + pos
+    const long long b = bp / npos;
+    x[t] = (double)out[bp * Rp + i] * sigma[b];
+  }
+}
+}  // namespace
+
+extern "C" int pot3d_fno_guess(const float *out, long long B, long long npos, int Rp, int R, const double *sigma,
+                               double *x, void *stream) {
+  if (B < 1 || npos < 1 || R < 1 || Rp < R) {
+    pot3d_set_error("pot3d_fno_guess: bad sizes");
+    return POT3D_ERR_ARG;
+  }
+  k_guess<<<grid_for(B * npos * R), 256, 0, (cudaStream_t)stream>>>(out, B, npos, Rp, R, sigma, x);
+  return pot3d_cuda_status(cudaGetLastError(), "pot3d_fno_guess");
+}

@@ -35,6 +35,11 @@ from .tc import tc_gemm
 F32, BF16 = 0, 1
 
 
+def _count():
+    from .tc import LAUNCHES
+    LAUNCHES[0] += 1
+
+
 def _ceil(n, m):
     return (n + m - 1) // m * m
 
@@ -49,6 +54,8 @@ def _L():
         L.pot3d_fno_colsum.argtypes = [vp, ll, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp]
         L.pot3d_fno_relmse.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, ll, C.c_int, C.c_float, vp, vp, vp]
         L.pot3d_fno_adam.argtypes = [vp, vp, vp, vp, vp, ll, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, vp]
+        L.pot3d_fno_inputs.argtypes = [vp, vp, ll, ll, vp, vp]
+        L.pot3d_fno_guess.argtypes = [vp, ll, ll, C.c_int, C.c_int, vp, vp, vp]
         L._fno_typed = True
     return L
 
@@ -68,6 +75,7 @@ def permute(inp, in_dims, out, out_dims, perm, add=False):
     idd = (C.c_longlong * 4)(*in_dims)
     odd = (C.c_longlong * 4)(*out_dims)
     pp = (C.c_int * 4)(*perm)
+    _count()
     _lib.check(_L().pot3d_fno_permute(C.c_void_p(inp.data_ptr()), _dt(inp), idd, C.c_void_p(out.data_ptr()),
                                       _dt(out), odd, pp, 1 if add else 0, _stream()))
     return out
@@ -87,6 +95,7 @@ def act(pre, C_, ldp, out, ldo, mode, grad=None, ldg=0):
         permute(pre, (1, 1, M, ldp), out, (1, 1, M, ldo), (0, 1, 2, 3))
         return out
     bwd = 1 if mode == "dgelu" else 0
+    _count()
     _lib.check(_L().pot3d_fno_gelu(C.c_void_p(pre.data_ptr()), M, C_, ldp,
                                    C.c_void_p(grad.data_ptr()) if grad is not None else None,
                                    _dt(grad) if grad is not None else 0, ldg, C.c_void_p(out.data_ptr()), _dt(out),
@@ -97,6 +106,7 @@ def act(pre, C_, ldp, out, ldo, mode, grad=None, ldg=0):
 def colsum(x, C_, ld, out, add=False, scratch=None):
     M = x.numel() // ld
     scratch = scratch if scratch is not None else new((64 * C_,), "f32")
+    _count()
     _lib.check(_L().pot3d_fno_colsum(C.c_void_p(x.data_ptr()), M, C_, ld, C.c_void_p(out.data_ptr()),
                                      1 if add else 0, C.c_void_p(scratch.data_ptr()), scratch.numel(), _stream()))
     return out
@@ -327,6 +337,7 @@ class FNO:
         npos = self.g.nph * self.g.nth
         grad = torch.empty_like(out)
         loss = new((B,), "f32")
+        _count()
         _lib.check(_L().pot3d_fno_relmse(C.c_void_p(out.data_ptr()), self.Rp, C.c_void_p(target.data_ptr()),
                                          _dt(target), B, npos, self.g.R, 1.0 / B, C.c_void_p(grad.data_ptr()),
                                          C.c_void_p(loss.data_ptr()), _stream()))
@@ -338,6 +349,7 @@ class FNO:
             gk = grads[k].contiguous().view(-1)
             assert gk.numel() == w.numel(), k
             wb = self.pb.get(k)
+            _count()
             _lib.check(_L().pot3d_fno_adam(C.c_void_p(w.data_ptr()), C.c_void_p(gk.data_ptr()),
                                            C.c_void_p(self.m1[k].data_ptr()), C.c_void_p(self.m2[k].data_ptr()),
                                            C.c_void_p(wb.data_ptr()) if wb is not None else None, w.numel(), lr, b1,
@@ -377,16 +389,21 @@ class FNO:
         m.pb = {k: v.to(torch.bfloat16).contiguous() for k, v in m.p.items() if v.dim() >= 2}
         return m
 
-    def predict(self, x, sigma):
-        """Initial guesses in the packed solver layout, FP64 [B, N]."""
+    def predict(self, x, sigma, out=None):
+        """Initial guesses in the packed solver layout, FP64 [B, N] (into
+        `out` when given); sigma: per-sample scales (host or FP64 device)."""
         import torch
         out = self.forward(x)
         B = x.shape[0]
         g = self.g
-        crop = new((B, g.nph, g.nth, g.R), "f32")
-        permute(out, (B, g.nph, g.nth, self.Rp), crop, (B, g.nph, g.nth, g.R), (0, 1, 2, 3))
-        sig = torch.tensor(np.asarray(sigma), dtype=torch.float64, device="cuda").view(B, 1)
-        return crop.view(B, -1).to(torch.float64) * sig
+        npos = g.nph * g.nth
+        sig = sigma if hasattr(sigma, "data_ptr") else torch.tensor(np.asarray(sigma, np.float64), device="cuda")
+        guess = out if out is not None else torch.empty((B, npos * g.R), dtype=torch.float64, device="cuda")
+        assert guess.dtype == torch.float64 and guess.is_contiguous() and guess.numel() == B * npos * g.R
+        _count()
+        _lib.check(_L().pot3d_fno_guess(C.c_void_p(out.data_ptr()), B, npos, self.Rp, g.R, C.c_void_p(sig.data_ptr()),
+                                        C.c_void_p(guess.data_ptr()), _stream()))
+        return guess
 
 
 def _bf():

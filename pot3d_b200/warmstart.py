@@ -57,6 +57,8 @@ class Inputs:
         B = br0n_dev.shape[0]
         g = self.model.g
         x = new((B, g.nph, g.nth, 64), "bf16")
+        from .tc import LAUNCHES
+        LAUNCHES[0] += 1
         _lib.check(_L().pot3d_fno_inputs(C.c_void_p(br0n_dev.data_ptr()), C.c_void_p(self.consts.data_ptr()), B,
                                          self.npos, C.c_void_p(x.data_ptr()), _stream()))
         return x
