@@ -155,7 +155,6 @@ constexpr int WSK = (WE - 1) + (WJT - 1);
 constexpr int WRIN = WSK + 1 + WPF;     // input plane ring (forward r32)
 constexpr int WROUT = 32;               // output plane ring (backward z32), > WSK
 constexpr int WXR = 4;                  // exchange ring depth (chunks)
-constexpr int WPU = 4;                  // prefetch distance (planes) of the fused update's FP64 loads
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
 static_assert(WROUT > WSK, "a plane is flushed after its last line wrote it");
 
@@ -179,15 +178,6 @@ struct WaveArgs {
   SolveState *st;
   int check;             // skip when the solve state is no longer running
   int nte, ntj, ntiles, ndiag, nsteps;
-  // forward sweep fused with the PCG update x += alpha p, r -= alpha q
-  double *x, *r;
-  const double *p, *q;
-  // backward sweep fused with r.z, the south-pole ring sums of z and ernorm
-  double *s1z;           // [nkc_u][NRP] ring partials read by the next stencil
-  double *partials;      // per-tile r.z
-  const double *dph;     // 1-based phi cell widths
-  double pl_i;
-  int nkc_u;
 };
 
 __device__ __forceinline__ void wave_publish(unsigned long long *p, unsigned epoch, float v) {
@@ -209,10 +199,6 @@ __device__ __forceinline__ void cp_async16(float4 *dst, const float4 *src, bool 
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(pred ? 16 : 0) : "memory");
 }
-__device__ __forceinline__ void cp_async_f64(double *dst, const double *src, bool pred) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(pred ? 8 : 0) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -227,15 +213,6 @@ struct WaveSmemF {                   // forward sweep
   int2 tile;
   int abort, ready, consumed;
 };
-struct WaveSmemU {                   // forward sweep fused with the PCG update
-  double upd[WPU][4][WAVE_THREADS];  // x, p, r, q of this line's planes, slot = plane % WPU
-  float lf[WPU][3][WAVE_THREADS];    // coefficient stream, slot = step % WPU
-  float rin[WRIN][WAVE_THREADS];     // FP32 r of the updated planes, slot = plane % WRIN
-  float y[2][WJT][WE + 1];
-  float ring[WXR][2][WCH][16];
-  int2 tile;
-  int abort, ready, consumed;
-};
 struct WaveSmemB {                   // backward sweep
   float4 ub[WPF][WAVE_THREADS];      // coefficient stream
   float yin[WPF][WAVE_THREADS];      // y stream
@@ -246,38 +223,15 @@ struct WaveSmemB {                   // backward sweep
   int abort, ready, consumed;
 };
 
-// Sweep variants: backward, forward, forward fused with the PCG update,
-// backward fused with r.z and the iteration's state update.
-enum { WV_BWD = 0, WV_FWD = 1, WV_FWDU = 2, WV_BWDZ = 3 };
-struct WaveSmemBZ {                  // backward sweep fused with r.z
-  float4 ub[WPF][WAVE_THREADS];
-  float yin[WPF][WAVE_THREADS];
-  float zout[WROUT][WAVE_THREADS];
-  double rr[WPF][WAVE_THREADS];      // r of the plane flushed at each step
-  float y[2][WJT][WE + 1];
-  float ring[WXR][2][WCH][16];
-  double red[(WAVE_THREADS + 32) / 32];
-  int2 tile;
-  int abort, ready, consumed, last;
-};
-
-template <int V>
+template <bool FWD>
 struct WaveSmemSel;
 template <>
-struct WaveSmemSel<WV_FWD> {
+struct WaveSmemSel<true> {
   using type = WaveSmemF;
 };
 template <>
-struct WaveSmemSel<WV_FWDU> {
-  using type = WaveSmemU;
-};
-template <>
-struct WaveSmemSel<WV_BWD> {
+struct WaveSmemSel<false> {
   using type = WaveSmemB;
-};
-template <>
-struct WaveSmemSel<WV_BWDZ> {
-  using type = WaveSmemBZ;
 };
 
 __device__ __forceinline__ void wave_bar_compute() { asm volatile("bar.sync 1, %0;" ::"n"(WAVE_THREADS) : "memory"); }
@@ -333,10 +287,9 @@ __device__ __forceinline__ bool wave_spin(const unsigned long long *p, unsigned 
 
 // Exchange warp: fills the face ring WXR chunks ahead of the compute warps.
 // Lane L serves face L >> 4, line L & 15, all WCH steps of a chunk.
-template <int V>
-__device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSmemSel<V>::type &S,
+template <bool FWD>
+__device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S,
                                               const WaveFaces &f, unsigned epoch, int nch) {
-  constexpr bool FWD = V == WV_FWD || V == WV_FWDU;
   const int lane = threadIdx.x & 31;
   const int face = lane >> 4, line = lane & 15;
   const unsigned long long *src = f.src[face] + line;
@@ -382,11 +335,9 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
   }
 }
 
-template <int V>
-__device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSel<V>::type &S, const WaveFaces &f,
+template <bool FWD>
+__device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S, const WaveFaces &f,
                                           unsigned epoch) {
-  constexpr bool FWD = V == WV_FWD || V == WV_FWDU, FUSED = V == WV_FWDU, RZ = V == WV_BWDZ;
-  constexpr int PF = FUSED ? WPU : WPF;  // stream prefetch distance (steps)
   const Geo &g = a.g;
   const int T = threadIdx.x;
   const int te = f.te, tj = f.tj, ti = f.ti;
@@ -423,62 +374,25 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
   const float4 *ub_p = a.ub + tbase + T;
   const float *ys_p = a.ys + tbase + T;
   const float *r_p = a.r32 + row;
-  // Fused update: this line's x, p, r, q of plane t arrive PF steps ahead;
-  // at step t the thread updates plane t (coalesced over the block) and
-  // feeds FP32 r into its own column of the plane ring.
-  const double alpha = FUSED ? *(volatile double *)&a.st->alpha : 0.0;
   auto issue = [&](int t) {
     const bool in_t = t < nsteps;
     if constexpr (FWD) {
       const float *l = lf_p + (size_t)(in_t ? t : 0) * 3 * WAVE_THREADS;
-      cp_async4(&S.lf[t & (PF - 1)][0][T], l, in_t);
-      cp_async4(&S.lf[t & (PF - 1)][1][T], l + WAVE_THREADS, in_t);
-      cp_async4(&S.lf[t & (PF - 1)][2][T], l + 2 * WAVE_THREADS, in_t);
+      cp_async4(&S.lf[t & (WPF - 1)][0][T], l, in_t);
+      cp_async4(&S.lf[t & (WPF - 1)][1][T], l + WAVE_THREADS, in_t);
+      cp_async4(&S.lf[t & (WPF - 1)][2][T], l + 2 * WAVE_THREADS, in_t);
       const bool rp = valid && t < npm2;
-      const long long off = row + (rp ? (long long)t * plane : 0);
-      if constexpr (FUSED) {
-        cp_async_f64(&S.upd[t & (WPU - 1)][0][T], a.x + off, rp);
-        cp_async_f64(&S.upd[t & (WPU - 1)][1][T], a.p + off, rp);
-        cp_async_f64(&S.upd[t & (WPU - 1)][2][T], a.r + off, rp);
-        cp_async_f64(&S.upd[t & (WPU - 1)][3][T], a.q + off, rp);
-      } else {
-        cp_async4(&S.rin[t % WRIN][T], a.r32 + off, rp);
-      }
+      cp_async4(&S.rin[t % WRIN][T], r_p + (rp ? (long long)t * plane : 0), rp);
     } else {
       cp_async16(&S.ub[t & (WPF - 1)][T], ub_p + (size_t)(in_t ? t : 0) * WAVE_THREADS, in_t);
       cp_async4(&S.yin[t & (WPF - 1)][T], ys_p + (size_t)(in_t ? nsteps - 1 - t : 0) * WAVE_THREADS, in_t);
-      if constexpr (RZ) {  // r of the plane flushed at step t
-        const int kd = npm2 + WSK - t;
-        const bool rp = valid && kd >= 0 && kd < npm2 && t > WSK;
-        cp_async_f64(&S.rr[t & (WPF - 1)][T], a.r + row + (rp ? (long long)kd * plane : 0), rp);
-      }
     }
     cp_async_commit();
   };
 #pragma unroll 1
-  for (int t = 0; t < PF; t++) issue(t);
+  for (int t = 0; t < WPF; t++) issue(t);
   float seam_y = 0.f;  // value at the line's first plane of the sweep
   float prev = 0.f;    // own value at the previous step
-  // Backward: at step t the plane npm2 + WSK - t is complete (its last line
-  // was written at step t-1); each thread stores its own line of it (one
-  // coalesced plane per step) and, fused, adds r.z and the ring sum of z.
-  const bool south = valid && jj == g.ntm2 - 1;
-  double rz = 0.0, s1 = 0.0;
-  int flushed_to = -1;  // last step whose plane was flushed
-  auto flush = [&](int t) {
-    if constexpr (!FWD) {
-      const int kd = npm2 + WSK - t;
-      if (kd < 0 || kd >= npm2 || t <= WSK) return;
-      flushed_to = t;
-      if (!valid) return;
-      const float z = S.zout[kd % WROUT][T];
-      a.z32[(long long)kd * plane + row] = z;
-      if constexpr (RZ) {
-        rz = fma(S.rr[t & (WPF - 1)][T], (double)z, rz);
-        if (south) s1 += __dmul_rn((double)z, a.dph[kd + 2]) * a.pl_i;
-      }
-    }
-  };
   int rslot = (WRIN - (sk % WRIN)) % WRIN;  // (t - sk) mod WRIN at t = 0
 #pragma unroll 1
   for (int c = 0; c < nch; c++) {
@@ -502,35 +416,28 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
     for (int u = 0; u < WCH; u++) {
       const int t = c * WCH + u;
       const float *yprev = &S.y[(t + 1) & 1][0][0];  // values of step t-1
-      cp_async_wait<PF - 1>();  // this step's group (and every older one) has landed
-      if constexpr (!FWD) flush(t);
+      if constexpr (!FWD) {
+        // flush the z32 plane whose last line was written at step t-1
+        const int kd = npm2 + WSK - t;
+        if (valid && kd >= 0 && kd < npm2 && t > WSK) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
+      }
+      cp_async_wait<WPF - 1>();  // this step's group (and every older one) has landed
       float v_in, c0, c1, c2, c3 = 0.f;
       if constexpr (FWD) {
-        if constexpr (FUSED) {
-          if (valid && t < npm2) {  // x += alpha p, r -= alpha q on plane t (src/pot3d.F90:4344-4347, FMA)
-            const double *u4 = &S.upd[t & (WPU - 1)][0][T];
-            const double xn = fma(alpha, u4[WAVE_THREADS], u4[0]);
-            const double rn = fma(-alpha, u4[3 * WAVE_THREADS], u4[2 * WAVE_THREADS]);
-            const long long off = row + (long long)t * plane;
-            a.x[off] = xn;
-            a.r[off] = rn;
-            S.rin[t % WRIN][T] = (float)rn;
-          }
-        }
-        c0 = S.lf[t & (PF - 1)][0][T];
-        c1 = S.lf[t & (PF - 1)][1][T];
-        c2 = S.lf[t & (PF - 1)][2][T];
+        c0 = S.lf[u & (WPF - 1)][0][T];
+        c1 = S.lf[u & (WPF - 1)][1][T];
+        c2 = S.lf[u & (WPF - 1)][2][T];
         v_in = S.rin[rslot][T];
       } else {
-        const float4 cf = S.ub[t & (WPF - 1)][T];
+        const float4 cf = S.ub[u & (WPF - 1)][T];
         c0 = cf.x;
         c1 = cf.y;
         c2 = cf.z;
         c3 = cf.w;
-        v_in = S.yin[t & (WPF - 1)][T];
+        v_in = S.yin[u & (WPF - 1)][T];
       }
       rslot = rslot + 1 == WRIN ? 0 : rslot + 1;
-      issue(t + PF);
+      issue(t + WPF);
       const int q = t - sk;
       if (valid && (unsigned)q < (unsigned)npm2) {
         const int kk = FWD ? q : npm2 - 1 - q;
@@ -566,34 +473,17 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
     }
     if (T == 0) *(volatile int *)&S.consumed = c + 1;
   }
-  cp_async_wait<0>();  // the rings are reused by the next tile
   if constexpr (!FWD) {  // the first plane completes at the last step
-    if (flushed_to < nsteps) flush(nsteps);
+    const int kd = npm2 + WSK - nsteps;
+    if (valid && kd >= 0 && kd < npm2) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
   }
-  if constexpr (RZ) {
-    // the tile's r.z in a fixed order (threads, then warps), and the ring
-    // sums of z of its south-pole radial points (the whole sum in chunk 0)
-    double v = warp_sum(rz);
-    if ((T & 31) == 0) S.red[T >> 5] = v;
-    wave_bar_compute();
-    if (T == 0) {
-      double tsum = 0.0;
-      for (int w = 0; w < WAVE_THREADS / 32; w++) tsum += S.red[w];
-      a.partials[ti] = tsum;
-    }
-    if (south) {
-      a.s1z[e] = s1;
-      for (int c = 1; c < a.nkc_u; c++) a.s1z[(long long)c * g.NRP + e] = 0.0;
-    }
-    wave_bar_compute();  // S.red is reused by the next tile
-  }
+  cp_async_wait<0>();  // the rings are reused by the next tile
   return true;
 }
 
-template <int V>
+template <bool FWD>
 __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) {
-  constexpr bool FWD = V == WV_FWD || V == WV_FWDU;
-  using Sm = typename WaveSmemSel<V>::type;
+  using Sm = typename WaveSmemSel<FWD>::type;
   extern __shared__ float4 wave_dyn[];
   Sm &S = *reinterpret_cast<Sm *>(wave_dyn);
   const bool xwarp = threadIdx.x >= WAVE_THREADS;
@@ -613,9 +503,9 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) 
     const WaveFaces f = wave_faces<FWD>(a, tile.x, tile.y);
     bool ok = true;
     if (xwarp)
-      wave_exchange<V>(a, S, f, epoch, (a.nsteps + WCH - 1) / WCH);
+      wave_exchange<FWD>(a, S, f, epoch, (a.nsteps + WCH - 1) / WCH);
     else
-      ok = wave_tile<V>(a, S, f, epoch);
+      ok = wave_tile<FWD>(a, S, f, epoch);
     if (!ok) S.abort = 1;
     __syncthreads();
     if (S.abort) {
@@ -627,30 +517,6 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) 
     }
   }
   __syncthreads();
-  if constexpr (V == WV_BWDZ) {
-    // The last block sums the tiles' r.z in tile order and updates the
-    // iteration's state (what k_update<UPD_ZDOT> does for the unfused sweeps).
-    if (threadIdx.x == 0) {
-      __threadfence();
-      S.last = atomicAdd(&a.ctl->done, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (S.last) {
-      __threadfence();
-      const bool upd = run && *(volatile int *)&a.st->status == ST_RUNNING;
-      double v = 0.0;
-      for (int q = threadIdx.x; q < a.ntiles; q += blockDim.x) v += __ldcg(a.partials + q);
-      const double total = block_sum<WAVE_THREADS + 32>(v, S.red);
-      if (threadIdx.x == 0) {
-        if (upd) pcg_rz_state(a.st, total);
-        atomicExch(&a.ctl->ticket, 0u);
-        atomicExch(&a.ctl->done, 0u);
-        __threadfence();
-        atomicAdd(&a.ctl->epoch, 1u);
-      }
-    }
-    return;
-  }
   if (threadIdx.x == 0) {
     __threadfence();
     if (atomicAdd(&a.ctl->done, 1u) == gridDim.x - 1) {  // last block: reset for the next sweep
@@ -740,11 +606,10 @@ struct DiluState {
   // wavefront sweeps
   unsigned long long *xe = nullptr, *xj = nullptr;
   float *lf = nullptr, *ys = nullptr;   // forward coefficients, intermediate y (tile-skewed)
-  double *rz_tile = nullptr;             // per-tile r.z of the fused backward sweep
   float4 *ub = nullptr;                  // backward coefficients (tile-skewed)
   float *seam_f = nullptr, *seam_b = nullptr;
   int nsteps = 0;
-  size_t wave_smem_f = 0, wave_smem_b = 0, wave_smem_u = 0, wave_smem_z = 0;
+  size_t wave_smem_f = 0, wave_smem_b = 0;
   int2 *order = nullptr;
   WaveCtl *ctl = nullptr;
   int nte = 0, ntj = 0, ntiles = 0, ndiag = 0, wave_blocks = 0;
@@ -787,7 +652,6 @@ static int wave_setup(Solver *s) {
   int st;
   if ((st = s->alloc((void **)&D->xe, 8 * nx)) || (st = s->alloc((void **)&D->xj, 8 * nx)) ||
       (st = s->alloc((void **)&D->order, sizeof(int2) * D->ntiles)) ||
-      (st = s->alloc((void **)&D->rz_tile, sizeof(double) * D->ntiles)) ||
       (st = s->alloc((void **)&D->lf, sizeof(float) * 3 * ns)) || (st = s->alloc((void **)&D->ys, sizeof(float) * ns)) ||
       (st = s->alloc((void **)&D->ub, sizeof(float4) * ns)) ||
       (st = s->alloc((void **)&D->seam_f, sizeof(float) * (size_t)g.ntm2 * g.NRP)) ||
@@ -814,27 +678,18 @@ static int wave_setup(Solver *s) {
   CK(cudaMemcpyAsync(D->ctl, &c0, sizeof(WaveCtl), cudaMemcpyHostToDevice, s->stream));
   D->wave_smem_f = sizeof(WaveSmemF);
   D->wave_smem_b = sizeof(WaveSmemB);
-  D->wave_smem_u = sizeof(WaveSmemU);
-  D->wave_smem_z = sizeof(WaveSmemBZ);
-  CK(cudaFuncSetAttribute(k_dilu_wave<WV_BWDZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_z));
-  CK(cudaFuncSetAttribute(k_dilu_wave<WV_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_f));
-  CK(cudaFuncSetAttribute(k_dilu_wave<WV_BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_b));
-  CK(cudaFuncSetAttribute(k_dilu_wave<WV_FWDU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_u));
-  int dev = 0, nsm = 0, occ_f = 0, occ_b = 0, occ_u = 0, occ_z = 0;
+  CK(cudaFuncSetAttribute(k_dilu_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_f));
+  CK(cudaFuncSetAttribute(k_dilu_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_b));
+  int dev = 0, nsm = 0, occ_f = 0, occ_b = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<WV_FWD>, WAVE_THREADS + 32, D->wave_smem_f));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<WV_BWD>, WAVE_THREADS + 32, D->wave_smem_b));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k_dilu_wave<WV_FWDU>, WAVE_THREADS + 32, D->wave_smem_u));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_z, k_dilu_wave<WV_BWDZ>, WAVE_THREADS + 32, D->wave_smem_z));
-  const int occ = std::max(1, std::min(std::min(occ_f, occ_z), std::min(occ_b, occ_u)));
-  D->wave_blocks = std::max(1, std::min(occ * nsm, D->ntiles));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_THREADS + 32, D->wave_smem_f));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_THREADS + 32, D->wave_smem_b));
+  D->wave_blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, D->ntiles));
   return POT3D_OK;
 }
 
-// variant: WV_FWD, WV_BWD, or WV_FWDU (forward fused with x += alpha p,
-// r -= alpha q on the solver's x, r, q and the given p).
-static void launch_wave(Solver *s, int variant, bool check, const double *p = nullptr) {
+static void launch_wave(Solver *s, bool fwd, bool check) {
   DiluState *D = s->dilu;
   WaveArgs a{};
   a.g = s->g;
@@ -856,23 +711,10 @@ static void launch_wave(Solver *s, int variant, bool check, const double *p = nu
   a.ntiles = D->ntiles;
   a.ndiag = D->ndiag;
   a.nsteps = D->nsteps;
-  a.x = s->d_x;
-  a.r = s->d_r;
-  a.p = p;
-  a.q = s->d_q;
-  a.s1z = s->d_s1z;
-  a.partials = D->rz_tile;
-  a.dph = s->m.dph;
-  a.pl_i = s->m.pl_i;
-  a.nkc_u = s->g.nkc_u;
-  if (variant == WV_FWD)
-    k_dilu_wave<WV_FWD><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_f, s->stream>>>(a);
-  else if (variant == WV_FWDU)
-    k_dilu_wave<WV_FWDU><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_u, s->stream>>>(a);
-  else if (variant == WV_BWDZ)
-    k_dilu_wave<WV_BWDZ><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_z, s->stream>>>(a);
+  if (fwd)
+    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_f, s->stream>>>(a);
   else
-    k_dilu_wave<WV_BWD><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_b, s->stream>>>(a);
+    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_b, s->stream>>>(a);
 }
 
 int dilu_setup(Solver *s) {
@@ -925,18 +767,9 @@ float *dilu_z32(Solver *s) { return s->dilu->z32; }
 int dilu_sweep_launches(Solver *s) { return s->dilu ? 2 : 0; }
 
 int dilu_sweeps(Solver *s, bool check_status) {
-  launch_wave(s, WV_FWD, check_status);
-  launch_wave(s, WV_BWD, check_status);
+  launch_wave(s, true, check_status);
+  launch_wave(s, false, check_status);
   return pot3d_cuda_status(cudaGetLastError(), "ILU(0) sweeps");
-}
-
-// One PCG iteration after the stencil: x += alpha p, r -= alpha q fused into
-// the forward sweep, z = (LU)^-1 (float)r, and r.z with the iteration's
-// ernorm and state fused into the backward sweep.
-int dilu_update_sweeps(Solver *s, const double *p) {
-  launch_wave(s, WV_FWDU, true, p);
-  launch_wave(s, WV_BWDZ, true);
-  return pot3d_cuda_status(cudaGetLastError(), "ILU(0) update, sweeps and r.z");
 }
 
 // Average device time of the forward and of the backward sweep over `reps`
@@ -951,9 +784,9 @@ int dilu_time(Solver *s, int reps, double ms[2]) {
   ms[0] = ms[1] = 0.0;
   for (int it = 0; it < reps; it++) {
     CK(cudaEventRecord(e[0], s->stream));
-    launch_wave(s, WV_FWD, false);
+    launch_wave(s, true, false);
     CK(cudaEventRecord(e[1], s->stream));
-    launch_wave(s, WV_BWD, false);
+    launch_wave(s, false, false);
     CK(cudaEventRecord(e[2], s->stream));
     CK(cudaEventSynchronize(e[2]));
     float a = 0.f, b = 0.f;

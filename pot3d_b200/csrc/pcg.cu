@@ -502,6 +502,7 @@ struct UpdateArgs {
   const double *q;
   const float *ai;
   const float *z32;       // ILU(0) output (ifprec=2); ai is then unused
+  float *r32;             // ifprec=2: FP32 copy of r for the sweeps
   double *s1z_part;       // [nkc][NRP]
   SolveState *st;
   double *partials;
@@ -602,6 +603,29 @@ __global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a)
   update_body<KIND, ZIN>(g, m, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// ifprec=2 half of the update: x += alpha p ; r -= alpha q ; r32 = (float)r
+// (the FP64->FP32 cast of prec_inv, src/pot3d.F90:5207-5209, fused).
+__global__ void __launch_bounds__(NTHR) k_update_r32(Geo g, UpdateArgs a) {
+  const volatile SolveState *vs = a.st;
+  if (vs->status != ST_RUNNING) return;
+  const double alpha = vs->alpha;
+  const long long n = g.Np;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; 2 * t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long id = 2 * t;
+    double2 xv = *reinterpret_cast<const double2 *>(a.x + id);
+    double2 rv = *reinterpret_cast<const double2 *>(a.r + id);
+    const double2 pv = __ldg(reinterpret_cast<const double2 *>(a.p + id));
+    const double2 qv = __ldg(reinterpret_cast<const double2 *>(a.q + id));
+    xv.x = fma(alpha, pv.x, xv.x);
+    xv.y = fma(alpha, pv.y, xv.y);
+    rv.x = fma(-alpha, qv.x, rv.x);
+    rv.y = fma(-alpha, qv.y, rv.y);
+    *reinterpret_cast<double2 *>(a.x + id) = xv;
+    *reinterpret_cast<double2 *>(a.r + id) = rv;
+    *reinterpret_cast<float2 *>(a.r32 + id) = make_float2((float)rv.x, (float)rv.y);
+  }
+}
 __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__restrict__ r32) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x)
@@ -1301,9 +1325,12 @@ int Solver::launch_iteration() {
     mp.m64[1] = mp.m64[0];
     if ((stm = tensor_map(sa.z32, false, &mp.m32[0]))) return stm;
     k_stencil<MODE_PCGZ><<<grid, NTHR, StageLayout<MODE_PCGZ>::smem, stream>>>(mp, g, m, sa);
-    // update, preconditioner and r.z in the two sweeps
-    int st = dilu_update_sweeps(this, ua.p);
+    ua.r32 = dilu_r32(this);
+    k_update_r32<<<grid1d(g.Np / 2), NTHR, 0, stream>>>(g, ua);
+    int st = dilu_sweeps(this, true);
     if (st) return st;
+    ua.z32 = dilu_z32(this);
+    k_update<UPD_ZDOT, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
   } else {
     if ((stm = tensor_map(d_r, true, &mp.m64[1]))) return stm;
     if ((stm = tensor_map(d_ai, false, &mp.m32[0]))) return stm;
@@ -1410,7 +1437,7 @@ int Solver::cgsolve_padded(bool zero_guess, int ncgmax, double epscg, int *ierr,
       graph_kind = ifprec;
     }
     const long long per_graph = 2LL * U;
-    const long long nodes_per_iter = (ifprec == 2) ? 1 + sweep_launches() : 2;
+    const long long nodes_per_iter = (ifprec == 2) ? 3 + sweep_launches() : 2;
     long long launched = per_graph;
     int last_seen = -1, stalls = 0;
     CK(cudaGraphLaunch(graph_exec, stream));

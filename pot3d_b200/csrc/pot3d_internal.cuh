@@ -88,26 +88,6 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 // Last-block pattern: every block stores its partial at slot b, the block
 // that arrives last sums all partials in index order (deterministic for a
 // fixed grid) and returns true in all its threads with the total in *total.
-// rho <- r.z of a PCG iteration (total), ncg + 1, ernorm (src/pot3d.F90:4430-4483)
-// and the solve status; beta = rho / rho_old.
-__device__ __forceinline__ void pcg_rz_state(SolveState *s, double total) {
-  s->rho_old = s->rho;
-  s->rho = total;
-  s->ncg = s->ncg + 1;
-  const double epssq = total / s->bdotb;
-  const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
-  s->epsn = epsn;
-  if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
-  if (epsn < s->epscg) {
-    s->status = ST_CONVERGED;
-  } else if (s->ncg >= s->ncgmax) {
-    s->status = ST_MAXIT;
-  } else if (!isfinite(epsn)) {
-    s->status = ST_BREAKDOWN;
-  }
-  s->beta = total / s->rho_old;
-}
-
 template <int NT>
 __device__ bool last_block_sum_at(double part, double *partials, unsigned int *counter, unsigned int nblocks,
                                   unsigned int b, double *total, double *sh) {

@@ -393,15 +393,18 @@ class FNO:
         """Initial guesses in the packed solver layout, FP64 [B, N] (into
         `out` when given); sigma: per-sample scales (host or FP64 device)."""
         import torch
-        out = self.forward(x)
+        y = self.forward(x)  # FP32 [B, nph, nth, Rp]
         B = x.shape[0]
         g = self.g
         npos = g.nph * g.nth
+        assert y.dtype == torch.float32 and y.is_contiguous() and y.numel() == B * npos * self.Rp
         sig = sigma if hasattr(sigma, "data_ptr") else torch.tensor(np.asarray(sigma, np.float64), device="cuda")
+        assert sig.dtype == torch.float64 and sig.numel() == B
         guess = out if out is not None else torch.empty((B, npos * g.R), dtype=torch.float64, device="cuda")
-        assert guess.dtype == torch.float64 and guess.is_contiguous() and guess.numel() == B * npos * g.R
+        if guess.dtype != torch.float64 or not guess.is_contiguous() or guess.numel() != B * npos * g.R:
+            raise ValueError("predict: out must be a contiguous FP64 tensor of B x N")
         _count()
-        _lib.check(_L().pot3d_fno_guess(C.c_void_p(out.data_ptr()), B, npos, self.Rp, g.R, C.c_void_p(sig.data_ptr()),
+        _lib.check(_L().pot3d_fno_guess(C.c_void_p(y.data_ptr()), B, npos, self.Rp, g.R, C.c_void_p(sig.data_ptr()),
                                         C.c_void_p(guess.data_ptr()), _stream()))
         return guess
 

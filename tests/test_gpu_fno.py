@@ -84,3 +84,27 @@ def test_fno_save_load_roundtrip(cuda, tmp_path):
     assert torch.equal(m2.predict(x, sig), p0)
     with pytest.raises(ValueError):
         FNO.load(path, grid_from_mesh(host.make_mesh(20, 21, 35)))
+
+
+def test_predict_is_the_scaled_cropped_output(cuda):
+    """The guess kernel writes sigma * output[..., :R] in the solver's packed
+    layout, into a caller's buffer when given."""
+    import torch
+    from pot3d_b200 import host
+    from pot3d_b200.fno import FNO, grid_from_mesh
+    mesh = host.make_mesh(20, 21, 33)
+    g = grid_from_mesh(mesh)
+    m = FNO(g, seed=5)
+    maps = []
+    for sd in (1, 2):
+        tn, pn, fi = host.synthetic_br(sd, 8, 2, 21, 33)
+        maps.append(host.br0_from_map(mesh, tn, pn, fi))
+    x, sig = m.inputs(maps)
+    y = m.forward(x).view(2, g.nph, g.nth, -1)[..., :g.R].double()
+    ref = (y * torch.tensor(sig, device="cuda").view(2, 1, 1, 1)).reshape(2, -1)
+    out = torch.full((2, g.nph * g.nth * g.R), -1.0, dtype=torch.float64, device="cuda")
+    got = m.predict(x, sig, out=out)
+    assert got.data_ptr() == out.data_ptr()
+    assert torch.equal(out, ref)
+    with pytest.raises(ValueError):
+        m.predict(x, sig, out=torch.empty(5, dtype=torch.float64, device="cuda"))
