@@ -30,6 +30,7 @@
 
 #include "pot3d_internal.cuh"
 #include "pot3d_solver.h"
+#include "tma.cuh"
 
 namespace pot3d {
 
@@ -118,29 +119,30 @@ __global__ void k_dilu_factor(LevelArgs a) {
 // lines; thread (el, jl) is skewed by s = el + jl steps (mirrored in the
 // backward sweep), so at step t it handles plane k = t - s and its
 // neighbours (e-1, j, k) and (e, j-1, k) were produced by the threads
-// (el-1, jl) and (el, jl-1) one step earlier: the block runs in lockstep,
-// one barrier per step, and exchanges them through shared memory.
+// (el-1, jl) and (el, jl-1) one step earlier: the 8 compute warps run in
+// lockstep, one named barrier per step, and exchange them through shared
+// memory.
 //
-// Memory traffic stays coalesced despite the skew:
-//  * the sweep's private streams (coefficients, the intermediate y) are
-//    stored in a tile-skewed layout [tile][step][thread], so one step of a
-//    block is one contiguous 1 KB run per float;
-//  * the padded-layout vectors shared with the other kernels (r32 in,
-//    z32 out) go through a ring of phi planes in shared memory: every
-//    thread loads (or stores) its own line of plane p at the same step, so
-//    each warp touches two 64-byte row segments, and reads (or writes) its
-//    ring entry at its skewed step.
+// Streams.  One elected thread moves everything a tile reads with the bulk
+// copy engine, a few steps ahead, into rings tracked by mbarriers: the
+// sweep's private streams (coefficients and the intermediate y, stored
+// tile-skewed as [tile][group of 4 steps][component][thread] float4 so a
+// group of a block is one contiguous copy) and, forward, the r32 input as
+// 16 x 16 x 4 boxes of phi planes (a 3-D TMA load, no multicast).  A thread
+// then reads 4 steps of a coefficient with one 128-bit shared load.  The
+// backward sweep's z32 output goes through a ring of phi planes: every
+// thread stores its own line of the plane completed at the previous step,
+// so each warp writes two 64-byte row segments.
 //
 // Across tile faces values travel as 64-bit words holding the FP32 value
 // and a sweep tag, indexed by the step at which the consumer needs them, so
-// the words of one face for 8 consecutive steps are one contiguous block;
-// the block fetches the next 8 steps' words one chunk ahead, one thread per
-// face waits for the chunk's last word and the others re-poll (bounded)
-// only words not yet visible.  Tiles are taken in the order of the tickets
-// of a global counter, sorted so that every tile's producers hold smaller
-// tickets: a block only waits for a tile owned by a running block, and the
-// kernel needs no co-residency.  The last block to finish resets the
-// counter and advances the tag.
+// the words of one face for 8 consecutive steps are one contiguous block; a
+// dedicated exchange warp polls them (bounded) into a ring ahead of the
+// compute warps.  Tiles are taken in the order of the tickets of a global
+// counter, sorted so that every tile's producers hold smaller tickets: a
+// block only waits for a tile owned by a running block, and the kernel
+// needs no co-residency.  The last block to finish resets the counter and
+// advances the tag.
 //
 // The FP32 coefficients are formed once, after the factorisation, with the
 // reference's operations (lusol's l = a/d of the lower entries and the FP32
@@ -148,14 +150,19 @@ __global__ void k_dilu_factor(LevelArgs a) {
 // the sweeps are bit-identical to it.
 // ============================================================================
 constexpr int WE = 16, WJT = 16;        // lines per tile in e and j
-constexpr int WAVE_THREADS = WE * WJT;  // one thread per line
+constexpr int WAVE_THREADS = WE * WJT;  // one thread per line (compute warps)
 constexpr int WCH = 8;                  // steps per exchange chunk
-constexpr int WPF = 8;                  // prefetch distance of the streams (steps, power of 2)
+constexpr int WG = 4;                   // steps per stream group (one float4 per thread and component)
+constexpr int WSL = 3;                  // stream group slots (groups g+1, g+2 in flight while g is read)
+constexpr int WPD = 2;                  // r32 plane groups issued ahead
 constexpr int WSK = (WE - 1) + (WJT - 1);
-constexpr int WRIN = WSK + 1 + WPF;     // input plane ring (forward r32)
+constexpr int WPG = 11;                 // r32 plane-group slots
 constexpr int WROUT = 32;               // output plane ring (backward z32), > WSK
 constexpr int WXR = 4;                  // exchange ring depth (chunks)
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
+constexpr uint32_t WAVE_MBAR_LIMIT = 1u << 26;
+static_assert(WCH % WG == 0, "a chunk is whole stream groups");
+static_assert(WG * WPG > WSK + (WG - 1) + WG * WPD, "a plane group's slot is free when it is reissued");
 static_assert(WROUT > WSK, "a plane is flushed after its last line wrote it");
 
 struct WaveCtl {
@@ -165,11 +172,10 @@ struct WaveCtl {
 
 struct WaveArgs {
   Geo g;
-  const float *r32;      // forward input (padded layout)
   float *z32;            // backward output (padded layout)
-  float *ys;             // intermediate y (tile-skewed, forward step order)
-  const float *lf;       // forward coefficients (tile-skewed, [c][thread], c = l_k, l_j, l_e)
-  const float4 *ub;      // backward coefficients (tile-skewed): u_e, u_j, u_k, dinv
+  float4 *ys;            // intermediate y, [tile][group][thread] (forward step groups)
+  const float4 *lf;      // forward coefficients [tile][group][l_k, l_j, l_e][thread]
+  const float4 *ub;      // backward coefficients [tile][group][u_e, u_j, u_k, dinv][thread]
   const float *seam_f;   // forward seam coefficient of the last plane, per line
   const float *seam_b;   // backward seam coupling of the first plane, per line
   unsigned long long *xe, *xj;  // e-face and j-face exchange words
@@ -178,6 +184,7 @@ struct WaveArgs {
   SolveState *st;
   int check;             // skip when the solve state is no longer running
   int nte, ntj, ntiles, ndiag, nsteps;
+  int pad;               // nsteps - (npm2 + WSK): idle steps, trailing forward, leading backward
 };
 
 __device__ __forceinline__ void wave_publish(unsigned long long *p, unsigned epoch, float v) {
@@ -189,36 +196,31 @@ __device__ __forceinline__ unsigned long long wave_load(const unsigned long long
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
   return w;
 }
-
-// Asynchronous copies global -> shared (zero-filled when !pred).
-__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool pred) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(pred ? 4 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_async16(float4 *dst, const float4 *src, bool pred) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(pred ? 16 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+// Bulk copy global -> shared (16-byte aligned, size a multiple of 16),
+// completing on the mbarrier.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
 
-struct WaveSmemF {                   // forward sweep
-  float lf[WPF][3][WAVE_THREADS];    // coefficient stream, slot = step % WPF
-  float rin[WRIN][WAVE_THREADS];     // r32 planes, slot = plane % WRIN
+struct alignas(128) WaveSmemF {      // forward sweep
+  float rin[WPG][WG][WJT][WE];       // r32 plane groups (TMA boxes), slot = plane group % WPG
+  float4 lf[WSL][3][WAVE_THREADS];   // coefficient groups
   float y[2][WJT][WE + 1];           // step parity, line values
   float ring[WXR][2][WCH][16];       // chunk % WXR, face (0: e, 1: j), step in chunk, line
+  uint64_t bar_s[WSL], bar_p[WPG];
   int2 tile;
   int abort, ready, consumed;
 };
-struct WaveSmemB {                   // backward sweep
-  float4 ub[WPF][WAVE_THREADS];      // coefficient stream
-  float yin[WPF][WAVE_THREADS];      // y stream
+struct alignas(128) WaveSmemB {      // backward sweep
+  float4 ub[WSL][4][WAVE_THREADS];   // coefficient groups
+  float4 yin[WSL][WAVE_THREADS];     // y groups
   float zout[WROUT][WAVE_THREADS];   // z32 planes, slot = plane % WROUT
   float y[2][WJT][WE + 1];
   float ring[WXR][2][WCH][16];
+  uint64_t bar_s[WSL], bar_p[1];
   int2 tile;
   int abort, ready, consumed;
 };
@@ -272,7 +274,7 @@ __device__ __forceinline__ bool wave_needed(const WaveArgs &a, const WaveFaces &
   const int el_c = face == 0 ? (FWD ? 0 : WE - 1) : line, jl_c = face == 0 ? line : (FWD ? 0 : WJT - 1);
   if (f.te * WE + el_c >= a.g.nrm2 || f.tj * WJT + jl_c >= a.g.ntm2) return false;
   const int sk_c = FWD ? el_c + jl_c : (WE - 1 - el_c) + (WJT - 1 - jl_c);
-  const int q = t - sk_c;
+  const int q = t - (FWD ? 0 : a.pad) - sk_c;
   return t < a.ndiag && q >= 0 && q < a.g.npm2;
 }
 __device__ __forceinline__ bool wave_spin(const unsigned long long *p, unsigned epoch, unsigned long long *w) {
@@ -336,8 +338,9 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
 }
 
 template <bool FWD>
-__device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S, const WaveFaces &f,
-                                          unsigned epoch) {
+__device__ __forceinline__ bool wave_tile(const WaveArgs &a, const CUtensorMap *rmap,
+                                          typename WaveSmemSel<FWD>::type &S, const WaveFaces &f, unsigned epoch,
+                                          int gbase, int qbase) {
   const Geo &g = a.g;
   const int T = threadIdx.x;
   const int te = f.te, tj = f.tj, ti = f.ti;
@@ -348,7 +351,10 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
   const int npm2 = g.npm2;
   const long long plane = (long long)g.ntm2 * g.NRP;
   const long long row = (long long)(valid ? jj : 0) * g.NRP + (valid ? e : 0);
-  const size_t tbase = (size_t)ti * a.nsteps * WAVE_THREADS;  // tile-skewed stream base
+  const int nsteps = a.nsteps;          // a multiple of WCH
+  const int shift = FWD ? 0 : a.pad;    // backward: leading idle steps, so its y groups align
+  const int G = nsteps / WG;            // stream groups
+  const int NQ = (npm2 + WG - 1) / WG;  // r32 plane groups
   const int te_out = FWD ? te + 1 : te - 1, tj_out = FWD ? tj + 1 : tj - 1;
   const bool pub_e = valid && (FWD ? el == WE - 1 : el == 0) && te_out >= 0 && te_out < a.nte;
   const bool pub_j = valid && (FWD ? jl == WJT - 1 : jl == 0) && tj_out >= 0 && tj_out < a.ntj;
@@ -359,41 +365,82 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
   unsigned long long *xe_out = a.xe + (size_t)ti * a.ndiag * 16 + jl - (size_t)(WE - 1) * 16;
   unsigned long long *xj_out = a.xj + (size_t)ti * a.ndiag * 16 + el - (size_t)(WJT - 1) * 16;
   const float seam_c = valid ? (FWD ? a.seam_f[row] : a.seam_b[row]) : 0.f;
-  const int nsteps = a.nsteps;
-  const int nch = (nsteps + WCH - 1) / WCH;
-  // ring entries this thread reads for its out-of-tile neighbours
+  const int nch = nsteps / WCH;
   const int ring_e = (0 * WCH) * 16 + jl, ring_j = (1 * WCH) * 16 + el;
   const int y_e = ext_e ? 0 : jl * (WE + 1) + (FWD ? el - 1 : el + 1);
   const int y_j = ext_j ? 0 : (FWD ? jl - 1 : jl + 1) * (WE + 1) + el;
 
-  // Streams: one copy group per step, issued WPF steps before it is read.
-  // Forward: the coefficients of step t+WPF and this line's r32 of plane
-  // t+WPF (read at the step t+WPF+s that handles it).  Backward: the
-  // coefficients and y of step t+WPF (y in reversed forward step order).
-  const float *lf_p = a.lf + tbase * 3 + T;
-  const float4 *ub_p = a.ub + tbase + T;
-  const float *ys_p = a.ys + tbase + T;
-  const float *r_p = a.r32 + row;
-  auto issue = [&](int t) {
-    const bool in_t = t < nsteps;
+  // Thread 0 issues the bulk copies; the mbarrier of a slot counts its uses
+  // over the block's tiles (gbase, qbase) for the wait parity.
+  auto issue_s = [&](int gi) {
+    const int slot = (gbase + gi) % WSL;
+    uint64_t *bar = &S.bar_s[slot];
     if constexpr (FWD) {
-      const float *l = lf_p + (size_t)(in_t ? t : 0) * 3 * WAVE_THREADS;
-      cp_async4(&S.lf[t & (WPF - 1)][0][T], l, in_t);
-      cp_async4(&S.lf[t & (WPF - 1)][1][T], l + WAVE_THREADS, in_t);
-      cp_async4(&S.lf[t & (WPF - 1)][2][T], l + 2 * WAVE_THREADS, in_t);
-      const bool rp = valid && t < npm2;
-      cp_async4(&S.rin[t % WRIN][T], r_p + (rp ? (long long)t * plane : 0), rp);
+      mbar_expect_tx(bar, 3 * WAVE_THREADS * 16);
+      bulk_load(&S.lf[slot][0][0], a.lf + ((size_t)ti * G + gi) * 3 * WAVE_THREADS, 3 * WAVE_THREADS * 16, bar);
     } else {
-      cp_async16(&S.ub[t & (WPF - 1)][T], ub_p + (size_t)(in_t ? t : 0) * WAVE_THREADS, in_t);
-      cp_async4(&S.yin[t & (WPF - 1)][T], ys_p + (size_t)(in_t ? nsteps - 1 - t : 0) * WAVE_THREADS, in_t);
+      mbar_expect_tx(bar, 5 * WAVE_THREADS * 16);
+      bulk_load(&S.ub[slot][0][0], a.ub + ((size_t)ti * G + gi) * 4 * WAVE_THREADS, 4 * WAVE_THREADS * 16, bar);
+      bulk_load(&S.yin[slot][0], a.ys + ((size_t)ti * G + (G - 1 - gi)) * WAVE_THREADS, WAVE_THREADS * 16, bar);
     }
-    cp_async_commit();
   };
-#pragma unroll 1
-  for (int t = 0; t < WPF; t++) issue(t);
+  auto issue_p = [&](int q) {
+    if constexpr (FWD) {
+      const int slot = (qbase + q) % WPG;
+      mbar_expect_tx(&S.bar_p[slot], WG * WJT * WE * 4);
+      tma_load_3d(&S.rin[slot][0][0][0], rmap, te * WE, tj * WJT, q * WG, &S.bar_p[slot]);
+    }
+  };
+  auto wait_s = [&](int gi) {
+    const int gg = gbase + gi;
+    return mbar_wait(&S.bar_s[gg % WSL], (uint32_t)(gg / WSL) & 1u, WAVE_MBAR_LIMIT);
+  };
+  auto wait_p = [&](int q) {
+    if constexpr (FWD) {
+      const int qq = qbase + q;
+      return mbar_wait(&S.bar_p[qq % WPG], (uint32_t)(qq / WPG) & 1u, WAVE_MBAR_LIMIT);
+    }
+    return true;
+  };
+  // On an abort every copy still in flight lands before the block moves on.
+  int issued_s = 0, issued_p = 0, waited_s = 0, waited_p = 0;
+  auto drain = [&]() {
+    if (T == 0) {
+      for (int gi = waited_s; gi < issued_s; gi++) wait_s(gi);
+      for (int q = waited_p; q < issued_p; q++) wait_p(q);
+    }
+  };
+
+  if (T == 0) {
+    for (int gi = 0; gi < WSL - 1 && gi < G; gi++) issue_s(gi);
+    for (int q = 0; FWD && q < WPD && q < NQ; q++) issue_p(q);
+  }
+  issued_s = min(WSL - 1, G);
+  issued_p = FWD ? min(WPD, NQ) : 0;
+
+  // Backward: at step t the plane npm2 + WSK - t is complete (its last line
+  // was written at step t-1); each thread stores its own line of it.
+  int flushed_to = -1;  // last step whose plane was flushed
+  auto flush = [&](int t) {
+    if constexpr (!FWD) {
+      const int kd = npm2 + WSK + shift - t;
+      if (kd < 0 || kd >= npm2 || t - shift <= WSK) return;
+      flushed_to = t;
+      if (valid) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
+    }
+  };
+
   float seam_y = 0.f;  // value at the line's first plane of the sweep
   float prev = 0.f;    // own value at the previous step
-  int rslot = (WRIN - (sk % WRIN)) % WRIN;  // (t - sk) mod WRIN at t = 0
+  // forward: plane p = t - sk of this line sits in slot (qbase + p / WG) % WPG,
+  // row p % WG (p < 0 at the first steps: the entry is never read)
+  int p_sub = 0, p_slot = 0;
+  {
+    const int p0 = -sk;  // plane at step 0
+    const int pg = (p0 - (WG - 1)) / WG;  // floor(p0 / WG) for p0 <= 0
+    p_sub = p0 - pg * WG;
+    p_slot = ((qbase + pg) % WPG + WPG) % WPG;
+  }
 #pragma unroll 1
   for (int c = 0; c < nch; c++) {
     {  // wait until the exchange warp has chunk c in the ring
@@ -408,87 +455,123 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, typename WaveSmemSe
       __threadfence_block();
     }
     if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) {  // uniform over the compute warps
-      cp_async_wait<0>();
+      drain();
       return false;
     }
     const float *ring = &S.ring[c % WXR][0][0][0];
 #pragma unroll
-    for (int u = 0; u < WCH; u++) {
-      const int t = c * WCH + u;
-      const float *yprev = &S.y[(t + 1) & 1][0][0];  // values of step t-1
-      if constexpr (!FWD) {
-        // flush the z32 plane whose last line was written at step t-1
-        const int kd = npm2 + WSK - t;
-        if (valid && kd >= 0 && kd < npm2 && t > WSK) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
+    for (int h = 0; h < WCH / WG; h++) {
+      const int gi = c * (WCH / WG) + h;
+      // the slot of group gi-1 was released by the barrier that ended it
+      if (T == 0) {
+        // the compute warps' reads of the slots being refilled are ordered
+        // (named barrier) before these async-proxy writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (gi + WSL - 1 < G) issue_s(gi + WSL - 1);
+        if (FWD && gi + WPD < NQ) issue_p(gi + WPD);
       }
-      cp_async_wait<WPF - 1>();  // this step's group (and every older one) has landed
-      float v_in, c0, c1, c2, c3 = 0.f;
+      issued_s = min(gi + WSL, G);
+      if (FWD) issued_p = min(gi + WPD + 1, NQ);
+      bool ok = wait_s(gi);
+      waited_s = gi + 1;
+      if (FWD && gi < NQ) {
+        ok = wait_p(gi) && ok;
+        waited_p = gi + 1;
+      }
+      if (!ok) S.abort = 1;  // acted on at the next chunk
+      const int sl = (gbase + gi) % WSL;
+      float4 c0, c1, c2, c3 = make_float4(0.f, 0.f, 0.f, 0.f), yin4 = c3;
       if constexpr (FWD) {
-        c0 = S.lf[u & (WPF - 1)][0][T];
-        c1 = S.lf[u & (WPF - 1)][1][T];
-        c2 = S.lf[u & (WPF - 1)][2][T];
-        v_in = S.rin[rslot][T];
+        c0 = S.lf[sl][0][T];
+        c1 = S.lf[sl][1][T];
+        c2 = S.lf[sl][2][T];
       } else {
-        const float4 cf = S.ub[u & (WPF - 1)][T];
-        c0 = cf.x;
-        c1 = cf.y;
-        c2 = cf.z;
-        c3 = cf.w;
-        v_in = S.yin[u & (WPF - 1)][T];
+        c0 = S.ub[sl][0][T];
+        c1 = S.ub[sl][1][T];
+        c2 = S.ub[sl][2][T];
+        c3 = S.ub[sl][3][T];
+        yin4 = S.yin[sl][T];
       }
-      rslot = rslot + 1 == WRIN ? 0 : rslot + 1;
-      issue(t + WPF);
-      const int q = t - sk;
-      if (valid && (unsigned)q < (unsigned)npm2) {
-        const int kk = FWD ? q : npm2 - 1 - q;
-        const float ne = ext_e ? ring[ring_e + u * 16] : yprev[y_e];
-        const float nj = ext_j ? ring[ring_j + u * 16] : yprev[y_j];
-        float y = v_in;
-        if (FWD) {
-          // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1)
-          if (kk == npm2 - 1) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
-          if (kk > 0) y = __fsub_rn(y, __fmul_rn(c0, prev));
-          if (cpl_j) y = __fsub_rn(y, __fmul_rn(c1, nj));
-          if (cpl_e) y = __fsub_rn(y, __fmul_rn(c2, ne));
-          if (kk == 0) seam_y = y;
-        } else {
-          // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv
-          if (cpl_e) y = __fsub_rn(y, __fmul_rn(c0, ne));
-          if (cpl_j) y = __fsub_rn(y, __fmul_rn(c1, nj));
-          if (kk < npm2 - 1) y = __fsub_rn(y, __fmul_rn(c2, prev));
-          if (kk == 0) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
-          y = __fmul_rn(y, c3);
-          if (kk == npm2 - 1) seam_y = y;
+      float y4[WG];
+#pragma unroll
+      for (int u = 0; u < WG; u++) {
+        const int t = gi * WG + u;
+        const int uc = h * WG + u;  // step within the chunk
+        const float *yprev = &S.y[(t + 1) & 1][0][0];  // values of step t-1
+        if constexpr (!FWD) flush(t);
+        const float k0 = u == 0 ? c0.x : u == 1 ? c0.y : u == 2 ? c0.z : c0.w;
+        const float k1 = u == 0 ? c1.x : u == 1 ? c1.y : u == 2 ? c1.z : c1.w;
+        const float k2 = u == 0 ? c2.x : u == 1 ? c2.y : u == 2 ? c2.z : c2.w;
+        const float k3 = u == 0 ? c3.x : u == 1 ? c3.y : u == 2 ? c3.z : c3.w;
+        // backward y: forward step nsteps-1-t, component 3-u of the group
+        float v_in = u == 0 ? yin4.w : u == 1 ? yin4.z : u == 2 ? yin4.y : yin4.x;
+        if constexpr (FWD) {
+          v_in = S.rin[p_slot][p_sub][jl][el];
+          if (++p_sub == WG) {
+            p_sub = 0;
+            p_slot = p_slot + 1 == WPG ? 0 : p_slot + 1;
+          }
         }
-        S.y[t & 1][jl][el] = y;
-        if constexpr (FWD)
-          a.ys[tbase + (size_t)t * WAVE_THREADS + T] = y;
-        else
-          S.zout[kk % WROUT][T] = y;
-        if (pub_e) wave_publish(xe_out + (size_t)t * 16, epoch, y);
-        if (pub_j) wave_publish(xj_out + (size_t)t * 16, epoch, y);
-        prev = y;
+        float y = 0.f;
+        const int q = t - shift - sk;
+        if (valid && (unsigned)q < (unsigned)npm2) {
+          const int kk = FWD ? q : npm2 - 1 - q;
+          const float ne = ext_e ? ring[ring_e + uc * 16] : yprev[y_e];
+          const float nj = ext_j ? ring[ring_j + uc * 16] : yprev[y_j];
+          y = v_in;
+          if (FWD) {
+            // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1)
+            if (kk == npm2 - 1) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
+            if (kk > 0) y = __fsub_rn(y, __fmul_rn(k0, prev));
+            if (cpl_j) y = __fsub_rn(y, __fmul_rn(k1, nj));
+            if (cpl_e) y = __fsub_rn(y, __fmul_rn(k2, ne));
+            if (kk == 0) seam_y = y;
+          } else {
+            // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv
+            if (cpl_e) y = __fsub_rn(y, __fmul_rn(k0, ne));
+            if (cpl_j) y = __fsub_rn(y, __fmul_rn(k1, nj));
+            if (kk < npm2 - 1) y = __fsub_rn(y, __fmul_rn(k2, prev));
+            if (kk == 0) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
+            y = __fmul_rn(y, k3);
+            if (kk == npm2 - 1) seam_y = y;
+          }
+          S.y[t & 1][jl][el] = y;
+          if constexpr (!FWD) S.zout[kk % WROUT][T] = y;
+          if (pub_e) wave_publish(xe_out + (size_t)t * 16, epoch, y);
+          if (pub_j) wave_publish(xj_out + (size_t)t * 16, epoch, y);
+          prev = y;
+        }
+        y4[u] = y;
+        wave_bar_compute();
       }
-      wave_bar_compute();
+      if constexpr (FWD) a.ys[((size_t)ti * G + gi) * WAVE_THREADS + T] = make_float4(y4[0], y4[1], y4[2], y4[3]);
     }
     if (T == 0) *(volatile int *)&S.consumed = c + 1;
   }
-  if constexpr (!FWD) {  // the first plane completes at the last step
-    const int kd = npm2 + WSK - nsteps;
-    if (valid && kd >= 0 && kd < npm2) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
+  if constexpr (!FWD) {  // the first plane completes at step npm2 + WSK + shift
+    if (flushed_to < npm2 + WSK + shift) flush(npm2 + WSK + shift);
   }
-  cp_async_wait<0>();  // the rings are reused by the next tile
   return true;
 }
 
 template <bool FWD>
-__global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) {
+__global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(const __grid_constant__ CUtensorMap rmap,
+                                                                    WaveArgs a) {
   using Sm = typename WaveSmemSel<FWD>::type;
-  extern __shared__ float4 wave_dyn[];
-  Sm &S = *reinterpret_cast<Sm *>(wave_dyn);
+  extern __shared__ unsigned char wave_dyn[];
+  Sm &S = *reinterpret_cast<Sm *>(wave_dyn + ((128 - (smem_u32(wave_dyn) & 127)) & 127));
   const bool xwarp = threadIdx.x >= WAVE_THREADS;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < WSL; q++) mbar_init(&S.bar_s[q], 1);
+    for (int q = 0; q < (FWD ? WPG : 1); q++) mbar_init(&S.bar_p[q], 1);
+    mbar_init_fence();
+    if (FWD) tma_prefetch_desc(&rmap);
+  }
+  __syncthreads();
   const unsigned epoch = *(volatile unsigned *)&a.ctl->epoch;
   const bool run = !(a.check && *(volatile int *)&a.st->status != ST_RUNNING);
+  const int G = a.nsteps / WG, NQ = (a.g.npm2 + WG - 1) / WG;
+  int gbase = 0, qbase = 0;  // bulk-copy groups of earlier tiles of this block
   while (run) {
     if (threadIdx.x == 0) {
       const unsigned t = atomicAdd(&a.ctl->ticket, 1u);
@@ -503,9 +586,9 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) 
     const WaveFaces f = wave_faces<FWD>(a, tile.x, tile.y);
     bool ok = true;
     if (xwarp)
-      wave_exchange<FWD>(a, S, f, epoch, (a.nsteps + WCH - 1) / WCH);
+      wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
     else
-      ok = wave_tile<FWD>(a, S, f, epoch);
+      ok = wave_tile<FWD>(a, &rmap, S, f, epoch, gbase, qbase);
     if (!ok) S.abort = 1;
     __syncthreads();
     if (S.abort) {
@@ -515,6 +598,8 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) 
       }
       break;
     }
+    gbase += G;
+    qbase += FWD ? NQ : 0;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -528,45 +613,47 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(WaveArgs a) 
   }
 }
 
-// Coefficient streams of the sweeps in the tile-skewed layout, formed once
-// from the factor with the reference's operations (Row7 operand order, FP32
-// division by the pivot); zero where a thread has no point at a step.
+// Coefficient streams of the sweeps in the tile-skewed group layout, formed
+// once from the factor with the reference's operations (Row7 operand order,
+// FP32 division by the pivot); zero where a thread has no point at a step.
 __global__ void k_wave_streams(Geo g, DevMesh m, const float *__restrict__ d, const float *__restrict__ dinv,
-                               int nte, int ntiles, int nsteps, float *__restrict__ lf, float4 *__restrict__ ub) {
-  const long long total = (long long)ntiles * nsteps * WAVE_THREADS;
+                               int nte, int ntiles, int nsteps, int pad, float4 *__restrict__ lf,
+                               float4 *__restrict__ ub) {
+  const int G = nsteps / WG;
+  const long long total = (long long)ntiles * G * WAVE_THREADS;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
        q += (long long)gridDim.x * blockDim.x) {
     const int T = (int)(q % WAVE_THREADS);
-    const long long r = q / WAVE_THREADS;
-    const int t = (int)(r % nsteps);
-    const int ti = (int)(r / nsteps);
+    const long long rr = q / WAVE_THREADS;
+    const int gi = (int)(rr % G);
+    const int ti = (int)(rr / G);
     const int te = ti % nte, tj = ti / nte;
     const int el = T & (WE - 1), jl = T / WE;
     const int e = te * WE + el, jj = tj * WJT + jl;
     const bool valid = e < g.nrm2 && jj < g.ntm2;
-    float l0 = 0.f, l1 = 0.f, l2 = 0.f;
-    float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int kf = t - (el + jl);
-    if (valid && kf >= 0 && kf < g.npm2) {  // forward point (e, jj, kf)
-      const Row7 c = row7(m, e + 2, jj + 2, kf + 2);
-      if (kf > 0) l0 = __fdiv_rn((float)c.a1, d[g.idx(e, jj, kf - 1)]);
-      if (jj > 0) l1 = __fdiv_rn((float)c.a2, d[g.idx(e, jj - 1, kf)]);
-      if (e > 0) l2 = __fdiv_rn((float)c.a3, d[g.idx(e - 1, jj, kf)]);
+    float l[3][WG] = {}, u[4][WG] = {};
+    for (int s = 0; s < WG; s++) {
+      const int t = gi * WG + s;
+      const int kf = t - (el + jl);
+      if (valid && kf >= 0 && kf < g.npm2) {  // forward point (e, jj, kf)
+        const Row7 c = row7(m, e + 2, jj + 2, kf + 2);
+        if (kf > 0) l[0][s] = __fdiv_rn((float)c.a1, d[g.idx(e, jj, kf - 1)]);
+        if (jj > 0) l[1][s] = __fdiv_rn((float)c.a2, d[g.idx(e, jj - 1, kf)]);
+        if (e > 0) l[2][s] = __fdiv_rn((float)c.a3, d[g.idx(e - 1, jj, kf)]);
+      }
+      const int qb = t - pad - ((WE - 1 - el) + (WJT - 1 - jl));
+      if (valid && qb >= 0 && qb < g.npm2) {  // backward point (e, jj, npm2-1-qb)
+        const int kb = g.npm2 - 1 - qb;
+        const Row7 c = row7(m, e + 2, jj + 2, kb + 2);
+        u[0][s] = e < g.nrm2 - 1 ? (float)c.a5 : 0.f;
+        u[1][s] = jj < g.ntm2 - 1 ? (float)c.a6 : 0.f;
+        u[2][s] = kb < g.npm2 - 1 ? (float)c.a7 : 0.f;
+        u[3][s] = dinv[g.idx(e, jj, kb)];
+      }
     }
-    const int qb = t - ((WE - 1 - el) + (WJT - 1 - jl));
-    if (valid && qb >= 0 && qb < g.npm2) {  // backward point (e, jj, npm2-1-qb)
-      const int kb = g.npm2 - 1 - qb;
-      const Row7 c = row7(m, e + 2, jj + 2, kb + 2);
-      u.x = e < g.nrm2 - 1 ? (float)c.a5 : 0.f;
-      u.y = jj < g.ntm2 - 1 ? (float)c.a6 : 0.f;
-      u.z = kb < g.npm2 - 1 ? (float)c.a7 : 0.f;
-      u.w = dinv[g.idx(e, jj, kb)];
-    }
-    const size_t base = ((size_t)ti * nsteps + t) * WAVE_THREADS;
-    lf[base * 3 + T] = l0;
-    lf[base * 3 + WAVE_THREADS + T] = l1;
-    lf[base * 3 + 2 * WAVE_THREADS + T] = l2;
-    ub[base + T] = u;
+    const size_t base = (size_t)ti * G + gi;
+    for (int c = 0; c < 3; c++) lf[(base * 3 + c) * WAVE_THREADS + T] = make_float4(l[c][0], l[c][1], l[c][2], l[c][3]);
+    for (int c = 0; c < 4; c++) ub[(base * 4 + c) * WAVE_THREADS + T] = make_float4(u[c][0], u[c][1], u[c][2], u[c][3]);
   }
 }
 
@@ -605,14 +692,13 @@ struct DiluState {
   std::vector<int> kk_lo, nkk, nblk;  // per level launch shape (factorisation)
   // wavefront sweeps
   unsigned long long *xe = nullptr, *xj = nullptr;
-  float *lf = nullptr, *ys = nullptr;   // forward coefficients, intermediate y (tile-skewed)
-  float4 *ub = nullptr;                  // backward coefficients (tile-skewed)
+  float4 *lf = nullptr, *ub = nullptr, *ys = nullptr;  // tile-skewed group streams
   float *seam_f = nullptr, *seam_b = nullptr;
-  int nsteps = 0;
-  size_t wave_smem_f = 0, wave_smem_b = 0;
   int2 *order = nullptr;
   WaveCtl *ctl = nullptr;
-  int nte = 0, ntj = 0, ntiles = 0, ndiag = 0, wave_blocks = 0;
+  CUtensorMap rmap;  // r32 in 16 x 16 x 4 boxes
+  int nte = 0, ntj = 0, ntiles = 0, ndiag = 0, nsteps = 0, wave_blocks = 0;
+  size_t wave_smem_f = 0, wave_smem_b = 0;
 };
 
 static void level_shape(const Geo &g, int l, int *kk_lo, int *nkk, int *nblk) {
@@ -645,19 +731,20 @@ static int wave_setup(Solver *s) {
   D->nte = (g.nrm2 + WE - 1) / WE;
   D->ntj = (g.ntm2 + WJT - 1) / WJT;
   D->ntiles = D->nte * D->ntj;
-  D->ndiag = g.npm2 + 16;
-  D->nsteps = g.npm2 + WSK;
+  D->nsteps = (g.npm2 + WSK + WCH - 1) / WCH * WCH;  // whole chunks (and stream groups)
+  D->ndiag = D->nsteps - (WSK / 2 - 1);               // consumer steps that receive face words
   const size_t nx = (size_t)D->ntiles * D->ndiag * 16;
-  const size_t ns = (size_t)D->ntiles * D->nsteps * WAVE_THREADS;
+  const size_t ng = (size_t)D->ntiles * (D->nsteps / WG) * WAVE_THREADS;  // float4 per stream component
   int st;
   if ((st = s->alloc((void **)&D->xe, 8 * nx)) || (st = s->alloc((void **)&D->xj, 8 * nx)) ||
       (st = s->alloc((void **)&D->order, sizeof(int2) * D->ntiles)) ||
-      (st = s->alloc((void **)&D->lf, sizeof(float) * 3 * ns)) || (st = s->alloc((void **)&D->ys, sizeof(float) * ns)) ||
-      (st = s->alloc((void **)&D->ub, sizeof(float4) * ns)) ||
+      (st = s->alloc((void **)&D->lf, sizeof(float4) * 3 * ng)) || (st = s->alloc((void **)&D->ys, sizeof(float4) * ng)) ||
+      (st = s->alloc((void **)&D->ub, sizeof(float4) * 4 * ng)) ||
       (st = s->alloc((void **)&D->seam_f, sizeof(float) * (size_t)g.ntm2 * g.NRP)) ||
       (st = s->alloc((void **)&D->seam_b, sizeof(float) * (size_t)g.ntm2 * g.NRP)) ||
       (st = s->alloc((void **)&D->ctl, sizeof(WaveCtl))))
     return st;
+  if ((st = encode_padded_map(g, D->r32, false, WE, WJT, WG, &D->rmap))) return st;
   // Tickets in order of the tile's first wavefront step WE te + WJT tj
   // (ties by te): a tile's producers (te-1, tj) and (te, tj-1) have smaller
   // keys; the backward sweep takes the tickets in reverse.
@@ -676,8 +763,8 @@ static int wave_setup(Solver *s) {
   CK(cudaMemsetAsync(D->seam_b, 0, sizeof(float) * (size_t)g.ntm2 * g.NRP, s->stream));
   const WaveCtl c0{0u, 0u, 1u, 0};  // tag 0 is the zeroed buffers': sweeps start at 1
   CK(cudaMemcpyAsync(D->ctl, &c0, sizeof(WaveCtl), cudaMemcpyHostToDevice, s->stream));
-  D->wave_smem_f = sizeof(WaveSmemF);
-  D->wave_smem_b = sizeof(WaveSmemB);
+  D->wave_smem_f = sizeof(WaveSmemF) + 128;  // + alignment slack of the dynamic base
+  D->wave_smem_b = sizeof(WaveSmemB) + 128;
   CK(cudaFuncSetAttribute(k_dilu_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_f));
   CK(cudaFuncSetAttribute(k_dilu_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_b));
   int dev = 0, nsm = 0, occ_f = 0, occ_b = 0;
@@ -693,7 +780,6 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   DiluState *D = s->dilu;
   WaveArgs a{};
   a.g = s->g;
-  a.r32 = D->r32;
   a.z32 = D->z32;
   a.ys = D->ys;
   a.lf = D->lf;
@@ -711,10 +797,11 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   a.ntiles = D->ntiles;
   a.ndiag = D->ndiag;
   a.nsteps = D->nsteps;
+  a.pad = D->nsteps - (s->g.npm2 + WSK);
   if (fwd)
-    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_f, s->stream>>>(a);
+    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_f, s->stream>>>(D->rmap, a);
   else
-    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_b, s->stream>>>(a);
+    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_b, s->stream>>>(D->rmap, a);
 }
 
 int dilu_setup(Solver *s) {
@@ -752,7 +839,8 @@ int dilu_setup(Solver *s) {
     pot3d_set_error("zero pivot in the ILU(0) factorisation at row " + std::to_string(piv));
     return POT3D_ERR_PIVOT;
   }
-  k_wave_streams<<<148 * 8, NTHR, 0, s->stream>>>(g, s->m, D->d, D->dinv, D->nte, D->ntiles, D->nsteps, D->lf, D->ub);
+  k_wave_streams<<<148 * 8, NTHR, 0, s->stream>>>(g, s->m, D->d, D->dinv, D->nte, D->ntiles, D->nsteps,
+                                                   D->nsteps - (g.npm2 + WSK), D->lf, D->ub);
   k_wave_seam<<<grid1d((long long)g.ntm2 * g.nrm2), NTHR, 0, s->stream>>>(g, s->m, D->d, D->seam_f, D->seam_b);
   return pot3d_cuda_status(cudaGetLastError(), "sweep coefficient streams");
 }

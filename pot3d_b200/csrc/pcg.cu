@@ -1010,6 +1010,29 @@ static EncodeTiledFn encode_tiled() {
   return fn;
 }
 
+// 3-D tensor map of a padded vector (i, j, k) = (NRP, ntm2, npm2) with a
+// box of bx x by x bz elements; zero fill outside the vector.
+int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, int bz, CUtensorMap *out) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) {
+    pot3d_set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return POT3D_ERR_CUDA;
+  }
+  const cuuint64_t es = fp64 ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)g.NRP, (cuuint64_t)g.ntm2, (cuuint64_t)g.npm2};
+  cuuint64_t strides[2] = {(cuuint64_t)g.NRP * es, (cuuint64_t)g.NRP * g.ntm2 * es};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(out, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                  const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    pot3d_set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return POT3D_ERR_CUDA;
+  }
+  return POT3D_OK;
+}
+
 // 3-D tensor map of a padded vector (i, j, k) = (NRP, ntm2, npm2) with the
 // stencil's box: 68 x 10 x 1 FP64 or 72 x 10 x 1 FP32.
 int Solver::tensor_map(const void *ptr, bool fp64, CUtensorMap *out) {
