@@ -239,7 +239,9 @@ def main():
     ap.add_argument("--ifprec", type=int, default=2)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"])
     ap.add_argument("--epscg", type=float, default=1e-9)
-    ap.add_argument("--cpu-sample-iters", type=int, default=20)
+    ap.add_argument("--cpu-sample-iters", type=int, default=0,
+                    help="PCG iterations of the CPU sample (0: 20 with the diagonal preconditioner, 6 with ILU(0), "
+                         "whose sequential sweeps take seconds per iteration)")
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="iteration count used to project the CPU sample (0: take it from a GPU solve)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -252,6 +254,8 @@ def main():
                     help="time the hot kernels briefly (stencil and update, or with --ifprec 2 the two "
                          "ILU(0) sweeps; used for ncu captures) and exit")
     args = ap.parse_args()
+    if args.cpu_sample_iters <= 0:
+        args.cpu_sample_iters = 6 if args.ifprec == 2 else 20
 
     if args.impl == "reference":
         return run_reference(args)
