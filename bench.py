@@ -390,7 +390,7 @@ def main():
     if args.ifprec == 2 and not args.no_plain:
         sp = Pot3dSolver(mesh, br0, option=opt, ifprec=1, precision="fp64", device=local)
         pt = []
-        for it in range(2):
+        for it in range(2 if args.warmup > 0 else 1):
             xt.zero_()
             rt.copy_(bt)
             torch.cuda.synchronize()
