@@ -430,7 +430,7 @@ def main():
         "config": {"workload": args.workload, "unknowns": N, "ifprec": args.ifprec, "precision": args.precision,
                    "initial_guess": "learned (FNO)" if model is not None else "zero",
                    "epscg": args.epscg, "seed": seed, "iterations": ncg, "parallelism": "replicas",
-                   "l2": f"working set ~{(40 if args.ifprec != 2 else 76) * N / 1e9:.1f} GB >> 126 MB L2, no flush"},
+                   "l2": f"working set ~{(52 if args.ifprec != 2 else 104) * N / 1e9:.1f} GB >> 126 MB L2, no flush"},
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roofline, "cpu_baseline": cb, "clocks": clk.summary(),
         "gpu_launches": launches, "true_residual": tres, "epsn": epsn, "plain_fp64": plain,
