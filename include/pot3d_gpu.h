@@ -192,14 +192,20 @@ int pot3d_gpu_energy_noalloc(int nr, int nt, int np, const double *rh, const dou
                              const double *sth, const double *dp, const double *dph,
                              const double *phi, double *w, void *stream);
 
-/* Batched solves: n independent cases (own mesh, br0 and pm_r1; ifprec=1,
- * FP64 PCG), each tiled kernel launch covering the tiles of every unfinished
+/* Batched solves: n independent cases (own mesh, br0 and pm_r1; FP64 PCG
+ * with the diagonal preconditioner, or ILU(0) through
+ * pot3d_gpu_batch_create_ex), each tiled kernel launch covering the tiles of every unfinished
  * case, with per-case convergence.  No counterpart in the reference, which
  * solves one case per run.  tk: stencil planes per block (0 = the per-case
  * default; see pot3d_gpu_batch_tune). */
 typedef struct pot3d_gpu_batch pot3d_gpu_batch;
 int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
                            const double *pm_r1s, int tk, pot3d_gpu_batch **out);
+/* The same with the preconditioner chosen: ifprec = 1 (diagonal, as above)
+ * or 2 (ILU(0) of every case, its two triangular sweeps run for all running
+ * cases by one wavefront kernel per direction). */
+int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                              const double *pm_r1s, int tk, int ifprec, pot3d_gpu_batch **out);
 /* Autotuner: times `iters` batched iterations for each candidate planes per
  * block, keeps the fastest (*best_tk; ms_out[c] = time of candidate c). */
 int pot3d_gpu_batch_tune(pot3d_gpu_batch *b, const int *candidates, int ncand, int iters, int *best_tk,

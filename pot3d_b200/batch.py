@@ -6,11 +6,11 @@ nr in {63, 95, 127}, nt in {91, 181}, np in {181, 361}, its own seeded Br map
 uniformly from [2, 3]; all are solved to the same ernorm tolerance by one
 BatchSolver, whose kernels cover every unfinished case per launch.
 
-    python -m pot3d_b200.batch [--n 48] [--seed 0] [--epscg 1e-9] [--out f.json]
+    python -m pot3d_b200.batch [--n 48] [--seed 0] [--epscg 1e-9] [--ifprec 1|2] [--out f.json]
 
 reports the batch time, per-case iterations, the autotuner's choice and the
-aggregate algorithmic HBM throughput (80 bytes per unknown per iteration,
-the FP64 diagonal-preconditioned PCG's minimum traffic), and compares with
+aggregate algorithmic HBM throughput (per unknown and iteration 80 bytes
+with the diagonal preconditioner, 136 with ILU(0)), and compares with
 the same cases solved one after another by the single-case solver.
 """
 from __future__ import annotations
@@ -27,7 +27,7 @@ from .host import PM_R1
 NR = (63, 95, 127)
 NT = (91, 181)
 NP = (181, 361)
-BYTES_PER_UNKNOWN_ITER = 80.0
+BYTES_PER_UNKNOWN_ITER = {1: 80.0, 2: 136.0}
 
 
 def batch_specs(n: int = 48, seed: int = 0):
@@ -59,12 +59,13 @@ def main(argv=None):
     ap.add_argument("--no-sequential", action="store_true")
     ap.add_argument("--repeats", type=int, default=2)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--ifprec", type=int, default=1, help="1: diagonal, 2: ILU(0) (batched wavefront sweeps)")
     a = ap.parse_args(argv)
     specs = batch_specs(a.n, a.seed)
     meshes, brs = batch_cases(specs)
     unknowns = [(m.nr - 2) * (m.nt - 2) * (m.np - 2) for m in meshes]
-    rep = {"n": a.n, "seed": a.seed, "epscg": a.epscg, "specs": specs}
-    with BatchSolver(meshes, brs, [PM_R1["ss"]] * a.n) as b:
+    rep = {"n": a.n, "seed": a.seed, "epscg": a.epscg, "ifprec": a.ifprec, "specs": specs}
+    with BatchSolver(meshes, brs, [PM_R1["ss"]] * a.n, ifprec=a.ifprec) as b:
         t0 = time.perf_counter()
         best, times = b.tune()
         rep["tune"] = {"best_planes_per_block": best, "ms": times, "seconds": time.perf_counter() - t0}
@@ -75,14 +76,15 @@ def main(argv=None):
         ncg = [i.ncg for i in b.infos]
         rep["batch"] = {"seconds": min(secs), "all_seconds": secs, "ierr": ierr, "ncg": ncg,
                         "kernel_launches": b.infos[0].kernel_launches}
-        moved = sum(BYTES_PER_UNKNOWN_ITER * u * k for u, k in zip(unknowns, ncg))
+        bpu = BYTES_PER_UNKNOWN_ITER[a.ifprec]
+        moved = sum(bpu * u * k for u, k in zip(unknowns, ncg))
         rep["batch"]["algorithmic_gbs"] = moved / min(secs) / 1e9
         rep["batch"]["max_case_iterations"] = max(ncg)
         sol0 = b.solution(0)
     if not a.no_sequential:
         tot, ncg1 = 0.0, []
         for q, (m, br) in enumerate(zip(meshes, brs)):
-            with Pot3dSolver(m, br) as s:
+            with Pot3dSolver(m, br, ifprec=a.ifprec) as s:
                 best_t = None
                 for _ in range(a.repeats):
                     x = np.zeros(s.N)
@@ -94,7 +96,7 @@ def main(argv=None):
                 if q == 0:
                     rep["case0_rel_diff_vs_single"] = float(np.linalg.norm(sol0 - x) / np.linalg.norm(x))
         rep["sequential"] = {"seconds": tot, "ncg": ncg1, "algorithmic_gbs":
-                             sum(BYTES_PER_UNKNOWN_ITER * u * k for u, k in zip(unknowns, ncg1)) / tot / 1e9}
+                             sum(bpu * u * k for u, k in zip(unknowns, ncg1)) / tot / 1e9}
         rep["speedup_vs_sequential"] = tot / rep["batch"]["seconds"]
     print(json.dumps({k: v for k, v in rep.items() if k != "specs"}))
     if a.out:

@@ -212,7 +212,7 @@ struct alignas(128) WaveSmemF {      // forward sweep
   float ring[WXR][2][WCH][16];       // chunk % WXR, face (0: e, 1: j), step in chunk, line
   uint64_t bar_s[WSL], bar_p[WPG];
   int2 tile;
-  int abort, ready, consumed;
+  int abort, ready, consumed, bcase;
 };
 struct alignas(128) WaveSmemB {      // backward sweep
   float4 ub[WSL][4][WAVE_THREADS];   // coefficient groups
@@ -222,7 +222,7 @@ struct alignas(128) WaveSmemB {      // backward sweep
   float ring[WXR][2][WCH][16];
   uint64_t bar_s[WSL], bar_p[1];
   int2 tile;
-  int abort, ready, consumed;
+  int abort, ready, consumed, bcase;
 };
 
 template <bool FWD>
@@ -613,6 +613,91 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(const __grid
   }
 }
 
+// Batched sweeps: the tiles of many independent cases in one persistent
+// kernel.  The ticket order interleaves the cases' tiles by wavefront key
+// (each case keeps its own topological order), so every case's wavefront
+// advances at once and the GPU is filled even where one case's wavefront is
+// narrow.  A case is read from a table (its arguments and r32 tensor map,
+// the map acquired for the tensormap proxy since it reached global memory by
+// a host copy); tiles of a case that is no longer running are skipped.
+struct alignas(64) WaveCase {
+  CUtensorMap rmap;
+  WaveArgs a;
+};
+
+template <bool FWD>
+__global__ void __launch_bounds__(WAVE_THREADS + 32, 2)
+    k_dilu_wave_batch(const WaveCase *__restrict__ cases, const int4 *__restrict__ order, int total, WaveCtl *ctl) {
+  using Sm = typename WaveSmemSel<FWD>::type;
+  extern __shared__ unsigned char wave_dyn[];
+  Sm &S = *reinterpret_cast<Sm *>(wave_dyn + ((128 - (smem_u32(wave_dyn) & 127)) & 127));
+  const bool xwarp = threadIdx.x >= WAVE_THREADS;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < WSL; q++) mbar_init(&S.bar_s[q], 1);
+    for (int q = 0; q < (FWD ? WPG : 1); q++) mbar_init(&S.bar_p[q], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const unsigned epoch = *(volatile unsigned *)&ctl->epoch;
+  int gbase = 0, qbase = 0;  // bulk-copy groups of earlier tiles of this block
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned t = atomicAdd(&ctl->ticket, 1u);
+      int c = -1;
+      int2 tl = make_int2(-1, -1);
+      if (t < (unsigned)total) {
+        const int4 o = order[FWD ? t : total - 1 - t];
+        const WaveArgs &ca = cases[o.x].a;
+        c = (ca.check && *(volatile int *)&ca.st->status != ST_RUNNING) ? -2 : o.x;  // -2: skip
+        tl = make_int2(o.y, o.z);
+        if (c >= 0) tma_acquire_desc(&cases[c].rmap);
+      }
+      S.bcase = c;
+      S.tile = tl;
+      S.abort = 0;
+      S.ready = 0;
+      S.consumed = 0;
+    }
+    __syncthreads();
+    const int c = S.bcase;
+    const int2 tile = S.tile;
+    if (tile.x < 0) break;
+    if (c < 0) {  // case finished: its tiles are skipped
+      __syncthreads();  // every thread has read S.bcase before thread 0 takes the next ticket
+      continue;
+    }
+    const WaveCase &C = cases[c];
+    const WaveArgs &a = C.a;
+    const WaveFaces f = wave_faces<FWD>(a, tile.x, tile.y);
+    bool ok = true;
+    if (xwarp)
+      wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
+    else
+      ok = wave_tile<FWD>(a, &C.rmap, S, f, epoch, gbase, qbase);
+    if (!ok) S.abort = 1;
+    __syncthreads();
+    if (S.abort) {
+      if (threadIdx.x == 0) {
+        atomicExch(&ctl->error, 1);
+        atomicExch(&a.st->status, ST_TIMEOUT);
+      }
+      break;
+    }
+    gbase += a.nsteps / WG;
+    qbase += FWD ? (a.g.npm2 + WG - 1) / WG : 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&ctl->done, 1u) == gridDim.x - 1) {  // last block: reset for the next sweep
+      atomicExch(&ctl->ticket, 0u);
+      atomicExch(&ctl->done, 0u);
+      __threadfence();
+      atomicAdd(&ctl->epoch, 1u);
+    }
+  }
+}
+
 // Coefficient streams of the sweeps in the tile-skewed group layout, formed
 // once from the factor with the reference's operations (Row7 operand order,
 // FP32 division by the pivot); zero where a thread has no point at a step.
@@ -776,7 +861,7 @@ static int wave_setup(Solver *s) {
   return POT3D_OK;
 }
 
-static void launch_wave(Solver *s, bool fwd, bool check) {
+static WaveArgs wave_args(Solver *s, bool check) {
   DiluState *D = s->dilu;
   WaveArgs a{};
   a.g = s->g;
@@ -798,10 +883,117 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   a.ndiag = D->ndiag;
   a.nsteps = D->nsteps;
   a.pad = D->nsteps - (s->g.npm2 + WSK);
+  return a;
+}
+
+static void launch_wave(Solver *s, bool fwd, bool check) {
+  DiluState *D = s->dilu;
+  const WaveArgs a = wave_args(s, check);
   if (fwd)
     k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_f, s->stream>>>(D->rmap, a);
   else
     k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_b, s->stream>>>(D->rmap, a);
+}
+
+// ---- batched sweeps over many cases -------------------------------------
+struct DiluBatch {
+  WaveCase *d_cases = nullptr;
+  int4 *d_order = nullptr;
+  WaveCtl *ctl = nullptr;
+  int total = 0, blocks = 0;
+  size_t smem_f = 0, smem_b = 0;
+};
+
+void dilu_batch_destroy(DiluBatch *B) {
+  if (!B) return;
+  if (B->d_cases) cudaFree(B->d_cases);
+  if (B->d_order) cudaFree(B->d_order);
+  if (B->ctl) cudaFree(B->ctl);
+  delete B;
+}
+
+int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch **out) {
+  *out = nullptr;
+  DiluBatch *B = new DiluBatch();
+  std::vector<WaveCase> h(n);
+  std::vector<int4> ord;
+  for (int q = 0; q < n; q++) {
+    DiluState *D = cases[q]->dilu;
+    if (!D) {
+      dilu_batch_destroy(B);
+      pot3d_set_error("batched ILU(0) sweeps: a case has no ILU(0) factor");
+      return POT3D_ERR_ARG;
+    }
+    h[q].rmap = D->rmap;
+    h[q].a = wave_args(cases[q], true);
+    for (int tj = 0; tj < D->ntj; tj++)
+      for (int te = 0; te < D->nte; te++) ord.push_back(make_int4(q, te, tj, 0));
+  }
+  // Every case keeps its producers-first order; the cases' wavefronts interleave.
+  std::stable_sort(ord.begin(), ord.end(), [](const int4 &x, const int4 &y) {
+    const int kx = WE * x.y + WJT * x.z, ky = WE * y.y + WJT * y.z;
+    if (kx != ky) return kx < ky;
+    return x.x != y.x ? x.x < y.x : x.y < y.y;
+  });
+  B->total = (int)ord.size();
+  int st;
+  auto fail = [&](int code) {
+    dilu_batch_destroy(B);
+    return code;
+  };
+  if ((st = pot3d_cuda_status(cudaMalloc(&B->d_cases, sizeof(WaveCase) * n), "cudaMalloc(batch sweep cases)")) ||
+      (st = pot3d_cuda_status(cudaMalloc(&B->d_order, sizeof(int4) * ord.size()), "cudaMalloc(batch sweep order)")) ||
+      (st = pot3d_cuda_status(cudaMalloc(&B->ctl, sizeof(WaveCtl)), "cudaMalloc(batch sweep control)")))
+    return fail(st);
+  // Sweep tags of the batch live above 2^31, the cases' own sweeps below it,
+  // so the shared exchange buffers never hold a word a later sweep accepts.
+  const WaveCtl c0{0u, 0u, 0x80000001u, 0};
+  if ((st = pot3d_cuda_status(
+           cudaMemcpyAsync(B->d_cases, h.data(), sizeof(WaveCase) * n, cudaMemcpyHostToDevice, stream),
+           "cudaMemcpy(batch sweep cases)")) ||
+      (st = pot3d_cuda_status(
+           cudaMemcpyAsync(B->d_order, ord.data(), sizeof(int4) * ord.size(), cudaMemcpyHostToDevice, stream),
+           "cudaMemcpy(batch sweep order)")) ||
+      (st = pot3d_cuda_status(cudaMemcpyAsync(B->ctl, &c0, sizeof(WaveCtl), cudaMemcpyHostToDevice, stream),
+                              "cudaMemcpy(batch sweep control)")) ||
+      (st = pot3d_cuda_status(cudaStreamSynchronize(stream), "batch sweep set-up")))
+    return fail(st);
+  B->smem_f = sizeof(WaveSmemF) + 128;
+  B->smem_b = sizeof(WaveSmemB) + 128;
+  int dev = 0, nsm = 0, occ_f = 0, occ_b = 0;
+  if ((st = pot3d_cuda_status(cudaFuncSetAttribute(k_dilu_wave_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)B->smem_f),
+                              "cudaFuncSetAttribute")) ||
+      (st = pot3d_cuda_status(cudaFuncSetAttribute(k_dilu_wave_batch<false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_b),
+                              "cudaFuncSetAttribute")) ||
+      (st = pot3d_cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) ||
+      (st = pot3d_cuda_status(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count")) ||
+      (st = pot3d_cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave_batch<true>,
+                                                                            WAVE_THREADS + 32, B->smem_f),
+                              "occupancy")) ||
+      (st = pot3d_cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave_batch<false>,
+                                                                            WAVE_THREADS + 32, B->smem_b),
+                              "occupancy")))
+    return fail(st);
+  B->blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, B->total));
+  *out = B;
+  return POT3D_OK;
+}
+
+// The two sweeps of every running case of the batch (z32 = (LU)^-1 r32).
+int dilu_batch_sweeps(DiluBatch *B, cudaStream_t stream) {
+  k_dilu_wave_batch<true><<<B->blocks, WAVE_THREADS + 32, B->smem_f, stream>>>(B->d_cases, B->d_order, B->total,
+                                                                              B->ctl);
+  k_dilu_wave_batch<false><<<B->blocks, WAVE_THREADS + 32, B->smem_b, stream>>>(B->d_cases, B->d_order, B->total,
+                                                                               B->ctl);
+  return pot3d_cuda_status(cudaGetLastError(), "batched ILU(0) sweeps");
+}
+
+// Clear the batch sweeps' ticket counter and advance their tag.
+int dilu_batch_reset(DiluBatch *B, cudaStream_t stream) {
+  k_wave_reset<<<1, 1, 0, stream>>>(B->ctl);
+  return pot3d_cuda_status(cudaGetLastError(), "k_wave_reset(batch)");
 }
 
 int dilu_setup(Solver *s) {

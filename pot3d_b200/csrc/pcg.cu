@@ -605,13 +605,12 @@ __global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a)
 
 // ifprec=2 half of the update: x += alpha p ; r -= alpha q ; r32 = (float)r
 // (the FP64->FP32 cast of prec_inv, src/pot3d.F90:5207-5209, fused).
-__global__ void __launch_bounds__(NTHR) k_update_r32(Geo g, UpdateArgs a) {
+__device__ __forceinline__ void update_r32_body(const Geo &g, const UpdateArgs &a, long long t0, long long stride) {
   const volatile SolveState *vs = a.st;
   if (vs->status != ST_RUNNING) return;
   const double alpha = vs->alpha;
   const long long n = g.Np;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; 2 * t < n;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = t0; 2 * t < n; t += stride) {
     const long long id = 2 * t;
     double2 xv = *reinterpret_cast<const double2 *>(a.x + id);
     double2 rv = *reinterpret_cast<const double2 *>(a.r + id);
@@ -625,6 +624,9 @@ __global__ void __launch_bounds__(NTHR) k_update_r32(Geo g, UpdateArgs a) {
     *reinterpret_cast<double2 *>(a.r + id) = rv;
     *reinterpret_cast<float2 *>(a.r32 + id) = make_float2((float)rv.x, (float)rv.y);
   }
+}
+__global__ void __launch_bounds__(NTHR) k_update_r32(Geo g, UpdateArgs a) {
+  update_r32_body(g, a, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__restrict__ r32) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -1823,18 +1825,24 @@ struct alignas(64) BatchInst {
   UpdateArgs ua[2];
   Geo g;
   DevMesh m;
-  unsigned off_s, off_u;
+  unsigned off_s, off_u, off_r;  // first block of the case in the stencil, update and r32-update grids
+  unsigned nb_r;                 // blocks of the case in the r32-update grid
 };
 
-__device__ __forceinline__ int batch_find(const BatchInst *__restrict__ in, int n, unsigned blk, bool upd) {
+enum { BATCH_STENCIL = 0, BATCH_UPDATE = 1, BATCH_R32 = 2 };
+__device__ __forceinline__ int batch_find(const BatchInst *__restrict__ in, int n, unsigned blk, int which) {
   int i = 0;
-  for (int q = 1; q < n; q++)
-    if ((upd ? in[q].off_u : in[q].off_s) <= blk) i = q;
+  for (int q = 1; q < n; q++) {
+    const unsigned o = which == BATCH_STENCIL ? in[q].off_s : which == BATCH_UPDATE ? in[q].off_u : in[q].off_r;
+    if (o <= blk) i = q;
+  }
   return i;
 }
 
+// MODE_PCG (diagonal preconditioner) or MODE_PCGZ (z from the ILU(0) sweeps).
+template <int MODE>
 __global__ void __launch_bounds__(NTHR, 2) k_stencil_batch(const BatchInst *__restrict__ in, int n, int par) {
-  const int i = batch_find(in, n, blockIdx.x, false);
+  const int i = batch_find(in, n, blockIdx.x, BATCH_STENCIL);
   const BatchInst &I = in[i];
   const Geo g = I.g;
   const DevMesh m = I.m;
@@ -1842,18 +1850,27 @@ __global__ void __launch_bounds__(NTHR, 2) k_stencil_batch(const BatchInst *__re
   const unsigned local = blockIdx.x - I.off_s;
   if (threadIdx.x == 0) {  // the thread that issues the TMA loads
     tma_acquire_desc(&I.maps[par].m64[0]);
-    tma_acquire_desc(&I.maps[par].m64[1]);
+    if (MODE == MODE_PCG) tma_acquire_desc(&I.maps[par].m64[1]);
     tma_acquire_desc(&I.maps[par].m32[0]);
   }
-  stencil_body<MODE_PCG>(I.maps[par], g, m, a, local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
+  stencil_body<MODE>(I.maps[par], g, m, a, local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
 }
 
+// UPD_ITER with the diagonal preconditioner, UPD_ZDOT after the ILU(0) sweeps.
+template <int KIND, bool ZIN>
 __global__ void __launch_bounds__(NTHR) k_update_batch(const BatchInst *__restrict__ in, int n, int par) {
-  const int i = batch_find(in, n, blockIdx.x, true);
+  const int i = batch_find(in, n, blockIdx.x, BATCH_UPDATE);
   const BatchInst &I = in[i];
   const Geo &g = I.g;
   const unsigned local = blockIdx.x - I.off_u;
-  update_body<UPD_ITER, false>(g, I.m, I.ua[par], local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
+  update_body<KIND, ZIN>(g, I.m, I.ua[par], local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
+}
+
+__global__ void __launch_bounds__(NTHR) k_update_r32_batch(const BatchInst *__restrict__ in, int n, int par) {
+  const int i = batch_find(in, n, blockIdx.x, BATCH_R32);
+  const BatchInst &I = in[i];
+  const unsigned local = blockIdx.x - I.off_r;
+  update_r32_body(I.g, I.ua[par], (long long)local * NTHR + threadIdx.x, (long long)I.nb_r * NTHR);
 }
 
 struct Batch {
@@ -1868,9 +1885,15 @@ struct Batch {
   cudaGraphExec_t graph = nullptr;
   std::vector<int> graph_act;  // the table the graph was captured for
   int U = 8;
-  int tk = 0;  // stencil planes per block (0 = per-case default)
+  int tk = 0;      // stencil planes per block (0 = per-case default)
+  int ifprec = 1;  // 1: diagonal preconditioner; 2: ILU(0) with batched wavefront sweeps
+  DiluBatch *wave = nullptr;
+  unsigned nblk_r = 0;
   ~Batch() {
     if (graph) cudaGraphExecDestroy(graph);
+    dilu_batch_destroy(wave);
+    for (Solver *s : inst)  // the cases run on the batch's stream, destroyed below
+      if (s && s->stream == stream) s->stream = nullptr;
     if (d_tab) cudaFree(d_tab);
     if (pin) cudaFreeHost(pin);
     if (ev0) cudaEventDestroy(ev0);
@@ -1898,7 +1921,8 @@ static void batch_set_tk(Batch &B, int tk) {
 // Build and upload the instance table of the cases in B.act.
 static int batch_table(Batch &B) {
   B.h_tab.assign(B.act.size(), BatchInst{});
-  unsigned os = 0, ou = 0;
+  unsigned os = 0, ou = 0, orr = 0;
+  const bool ilu = B.ifprec == 2;
   for (size_t t = 0; t < B.act.size(); t++) {
     Solver &s = *B.inst[B.act[t]];
     BatchInst &I = B.h_tab[t];
@@ -1928,18 +1952,33 @@ static int batch_table(Batch &B) {
       ua.st = s.d_state;
       ua.partials = s.d_partials;
       int st;
-      if ((st = s.tensor_map(pold, true, &I.maps[par].m64[0])) || (st = s.tensor_map(s.d_r, true, &I.maps[par].m64[1])) ||
-          (st = s.tensor_map(s.d_ai, false, &I.maps[par].m32[0])))
-        return st;
+      if (ilu) {  // the operands of launch_iteration's ifprec=2 branch
+        sa.z32 = dilu_z32(&s);
+        ua.z32 = dilu_z32(&s);
+        ua.r32 = dilu_r32(&s);
+        if ((st = s.tensor_map(pold, true, &I.maps[par].m64[0])) ||
+            (st = s.tensor_map(sa.z32, false, &I.maps[par].m32[0])))
+          return st;
+        I.maps[par].m64[1] = I.maps[par].m64[0];
+      } else {
+        if ((st = s.tensor_map(pold, true, &I.maps[par].m64[0])) ||
+            (st = s.tensor_map(s.d_r, true, &I.maps[par].m64[1])) ||
+            (st = s.tensor_map(s.d_ai, false, &I.maps[par].m32[0])))
+          return st;
+      }
       I.maps[par].m32[1] = I.maps[par].m32[2] = I.maps[par].m32[0];
     }
     I.off_s = os;
     I.off_u = ou;
+    I.off_r = orr;
+    I.nb_r = (unsigned)std::max(1LL, std::min((s.g.Np / 2 + NTHR - 1) / NTHR, 148LL * 4));
     os += (unsigned)s.g.nit * s.g.njt * s.g.nkc;
     ou += (unsigned)s.g.nit * s.g.njt * s.g.nkc_u;
+    orr += ilu ? I.nb_r : 0;
   }
   B.nblk_s = os;
   B.nblk_u = ou;
+  B.nblk_r = orr;
   if (B.act.empty()) return POT3D_OK;
   return pot3d_cuda_status(
       cudaMemcpyAsync(B.d_tab, B.h_tab.data(), sizeof(BatchInst) * B.act.size(), cudaMemcpyHostToDevice, B.stream),
@@ -1968,17 +2007,43 @@ static int batch_init(Batch &B, int ncgmax, double epscg) {
     ua.s1z_part = s.d_s1z;
     ua.st = s.d_state;
     ua.partials = s.d_partials;
-    k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
-    k_update<UPD_INIT, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+    if (B.ifprec == 2) {
+      // bdotb = b . M^-1 b and the initial z, rho as cgsolve_padded does,
+      // with the case's own (unbatched) sweeps
+      int st;
+      if ((st = dilu_reset(&s))) return st;
+      ua.z32 = dilu_z32(&s);
+      k_cast_r32<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_r, dilu_r32(&s));
+      if ((st = dilu_sweeps(&s, false))) return st;
+      k_update<UPD_BDOTB, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      k_cast_r32<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_r, dilu_r32(&s));
+      if ((st = dilu_sweeps(&s, false))) return st;
+      k_update<UPD_INIT, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+    } else {
+      k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      k_update<UPD_INIT, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+    }
+  }
+  if (B.ifprec == 2) {
+    int st;
+    if ((st = dilu_batch_reset(B.wave, B.stream))) return st;
   }
   return pot3d_cuda_status(cudaGetLastError(), "batch_init");
 }
 
 static void batch_iteration(Batch &B, int par) {
   const int n = (int)B.act.size();
-  k_stencil_batch<<<B.nblk_s, NTHR, StageLayout<MODE_PCG>::smem, B.stream>>>(B.d_tab, n, par);
-  k_update_batch<<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+  if (B.ifprec == 2) {  // launch_iteration's ifprec=2 sequence, every running case per launch
+    k_stencil_batch<MODE_PCGZ><<<B.nblk_s, NTHR, StageLayout<MODE_PCGZ>::smem, B.stream>>>(B.d_tab, n, par);
+    k_update_r32_batch<<<B.nblk_r, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+    dilu_batch_sweeps(B.wave, B.stream);
+    k_update_batch<UPD_ZDOT, true><<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+  } else {
+    k_stencil_batch<MODE_PCG><<<B.nblk_s, NTHR, StageLayout<MODE_PCG>::smem, B.stream>>>(B.d_tab, n, par);
+    k_update_batch<UPD_ITER, false><<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+  }
 }
+static int batch_launches_per_iteration(const Batch &B) { return B.ifprec == 2 ? 5 : 2; }
 
 // Capture 2U batched iterations of the current table into B.graph.
 static int batch_capture(Batch &B) {
@@ -2022,8 +2087,8 @@ struct pot3d_gpu_batch {
   pot3d::Batch b;
 };
 
-extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
-                                      const double *pm_r1s, int tk, pot3d_gpu_batch **out) {
+extern "C" int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                                         const double *pm_r1s, int tk, int ifprec, pot3d_gpu_batch **out) {
   using namespace pot3d;
   if (n < 1 || !meshes || !br0s || !pm_r1s || !out) {
     pot3d_set_error("pot3d_gpu_batch_create: invalid arguments");
@@ -2033,9 +2098,14 @@ extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const d
     pot3d_set_error("pot3d_gpu_batch_create: planes per block must be 0 or in [8, 512]");
     return POT3D_ERR_ARG;
   }
+  if (ifprec != 1 && ifprec != 2) {
+    pot3d_set_error("pot3d_gpu_batch_create: ifprec must be 1 (diagonal) or 2 (ILU(0))");
+    return POT3D_ERR_ARG;
+  }
   *out = nullptr;
   pot3d_gpu_batch *h = new pot3d_gpu_batch();
   Batch &B = h->b;
+  B.ifprec = ifprec;
   int st = pot3d_cuda_status(cudaStreamCreate(&B.stream), "cudaStreamCreate");
   if (!st) st = pot3d_cuda_status(cudaEventCreate(&B.ev0), "cudaEventCreate");
   if (!st) st = pot3d_cuda_status(cudaEventCreate(&B.ev1), "cudaEventCreate");
@@ -2044,7 +2114,7 @@ extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const d
   for (int q = 0; q < n && !st; q++) {
     Solver *s = new Solver();
     B.inst.push_back(s);
-    st = s->setup(&meshes[q], br0s[q], nullptr, pm_r1s[q], 1, POT3D_FP64);
+    st = s->setup(&meshes[q], br0s[q], nullptr, pm_r1s[q], ifprec, POT3D_FP64);
     if (!st) {
       s->tk_default = s->g.tk;
       s->nkc_default = s->g.nkc;
@@ -2054,12 +2124,23 @@ extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const d
         st = s->alloc((void **)&s->d_partials, sizeof(double) * need);
     }
   }
-  // the cases' setup ran on their own streams
+  // the cases' setup ran on their own streams; from now on they run on the batch's
   if (!st) st = pot3d_cuda_status(cudaDeviceSynchronize(), "batch setup");
+  for (Solver *s : B.inst)
+    if (!st && s->stream && s->stream != B.stream) {
+      cudaStreamDestroy(s->stream);
+      s->stream = B.stream;
+    }
   if (!st)
-    st = pot3d_cuda_status(cudaFuncSetAttribute(k_stencil_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    st = pot3d_cuda_status(cudaFuncSetAttribute(k_stencil_batch<MODE_PCG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 StageLayout<MODE_PCG>::smem),
                            "cudaFuncSetAttribute(k_stencil_batch)");
+  if (!st)
+    st = pot3d_cuda_status(cudaFuncSetAttribute(k_stencil_batch<MODE_PCGZ>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                StageLayout<MODE_PCGZ>::smem),
+                           "cudaFuncSetAttribute(k_stencil_batch)");
+  if (!st && ifprec == 2) st = dilu_batch_setup(B.inst.data(), n, B.stream, &B.wave);
   if (st) {
     delete h;
     return st;
@@ -2067,6 +2148,11 @@ extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const d
   batch_set_tk(B, tk);
   *out = h;
   return POT3D_OK;
+}
+
+extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                                      const double *pm_r1s, int tk, pot3d_gpu_batch **out) {
+  return pot3d_gpu_batch_create_ex(n, meshes, br0s, pm_r1s, tk, 1, out);
 }
 
 // Autotuner: times `iters` batched iterations of all cases for each candidate
@@ -2155,7 +2241,7 @@ extern "C" int pot3d_gpu_batch_solve(pot3d_gpu_batch *h, int ncgmax, double epsc
       if ((st = batch_table(B)) || (st = batch_capture(B))) return st;
     }
     CK(cudaGraphLaunch(B.graph, B.stream));
-    launches += 4LL * B.U;
+    launches += 2LL * B.U * batch_launches_per_iteration(B);
     if ((st = batch_poll(B))) return st;
   }
   CK(cudaEventRecord(B.ev1, B.stream));

@@ -92,10 +92,17 @@ float *dilu_z32(Solver *s);   // FP32 output z = (LU)^-1 r32
 int dilu_sweeps(Solver *s, bool check_status);
 int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, int bz, CUtensorMap *out);
 int dilu_reset(Solver *s);
-int dilu_status(Solver *s);
-int dilu_time(Solver *s, int reps, double ms[2]);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
+int dilu_status(Solver *s);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
+int dilu_time(Solver *s, int reps, double ms[2]);
 int dilu_diag(Solver *s, float *d_host, float *dinv_host);
 int dilu_sweep_launches(Solver *s);
+// Batched sweeps over many cases (dilu.cu): one kernel per direction covers
+// the tiles of every running case.
+struct DiluBatch;
+int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch **out);
+int dilu_batch_sweeps(DiluBatch *b, cudaStream_t stream);
+int dilu_batch_reset(DiluBatch *b, cudaStream_t stream);
+void dilu_batch_destroy(DiluBatch *b);
 
 
 // Kernel launch helpers shared between translation units.

@@ -165,10 +165,12 @@ class BatchSolver:
     """Many independent PCG solves (own grid, Br map and outer radius each)
     advanced together by the batched kernels: every launch covers the tiles of
     all unfinished cases, each case stops at its own ernorm criterion.  FP64
-    PCG with the diagonal preconditioner (ifprec=1), zero initial guess.
+    PCG with the diagonal preconditioner (ifprec=1) or ILU(0) (ifprec=2: both
+    triangular sweeps of all cases run in one wavefront kernel per
+    direction), zero initial guess.
     """
 
-    def __init__(self, meshes, br0s, pm_r1s, tk: int = 0):
+    def __init__(self, meshes, br0s, pm_r1s, tk: int = 0, ifprec: int = 1):
         if not (len(meshes) == len(br0s) == len(pm_r1s)) or not meshes:
             raise ValueError("meshes, br0s and pm_r1s must be non-empty and of equal length")
         n = len(meshes)
@@ -182,10 +184,11 @@ class BatchSolver:
         self._brp = (C.POINTER(C.c_double) * n)(*[dptr(b) for b in self._br])
         self._r1 = np.ascontiguousarray(pm_r1s, dtype=np.float64)
         h = C.c_void_p()
-        check(_lib.lib().pot3d_gpu_batch_create(n, self._mcs, self._brp, dptr(self._r1), tk, C.byref(h)))
+        check(_lib.lib().pot3d_gpu_batch_create_ex(n, self._mcs, self._brp, dptr(self._r1), tk, ifprec, C.byref(h)))
         self._h = h
         self.n = n
         self.tk = tk
+        self.ifprec = ifprec
         self.infos = None
         self.seconds = None
 

@@ -26,8 +26,8 @@ def _cases():
     return out
 
 
-def _single(mesh, br0, epscg):
-    with Pot3dSolver(mesh, br0) as s:
+def _single(mesh, br0, epscg, ifprec=1):
+    with Pot3dSolver(mesh, br0, ifprec=ifprec) as s:
         x = np.zeros(s.N)
         r = s.rhs()
         ierr = s.cgsolve(x, r, epscg=epscg)
@@ -84,3 +84,30 @@ def test_batch_rejects_bad_arguments(cuda):
     with BatchSolver([mesh], [br0], [1.0]) as b:
         with pytest.raises(Pot3dError):
             b.tune(candidates=(4,))
+
+
+def test_ilu_batch_matches_single_ilu_solves_bitwise(cuda):
+    """ILU(0) batch: the stencil, update and r.z run the single-case bodies on
+    the same tiles and the batched sweeps compute every value as the
+    single-case sweeps do, so iterations and solutions are bit-identical."""
+    cases = _cases()
+    with BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * len(cases), ifprec=2) as b:
+        for rep in range(2):  # the sweeps' tickets and tags carry over between solves
+            ierr = b.solve(epscg=1e-10)
+            assert ierr == [0] * len(cases)
+            ncgs = [i.ncg for i in b.infos]
+            for q, (mesh, br0) in enumerate(cases):
+                e1, n1, x1 = _single(mesh, br0, 1e-10, ifprec=2)
+                assert e1 == 0 and n1 == ncgs[q]
+                assert np.array_equal(b.solution(q), x1)
+        diag = BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * len(cases))
+        diag.solve(epscg=1e-10)
+        assert all(i.ncg < j.ncg for i, j in zip(b.infos, diag.infos))
+        diag.close()
+
+
+def test_batch_rejects_bad_preconditioner(cuda):
+    from pot3d_b200._lib import Pot3dError
+    mesh, br0 = _cases()[0]
+    with pytest.raises(Pot3dError):
+        BatchSolver([mesh], [br0], [1.0], ifprec=3)
