@@ -152,6 +152,16 @@ int pot3d_gpu_finalize_phi(pot3d_gpu_solver *s, const double *x, double *phi);
  * ghosts; w = {W_r, W_t, W_p}. */
 int pot3d_gpu_energy(pot3d_gpu_solver *s, const double *phi, double w[3]);
 
+/* The post-solve passes of the reference's main program in one device
+ * call: potfld's phi finalisation (src/pot3d.F90:3966-3969), getb
+ * (:6187-6233) and magnetic_energy (:6235-6321), from the interior solution
+ * x (host, N).  phi (nr,nt,np), br (nrm1,nt,np), bt (nr,ntm1,np),
+ * bp (nr,nt,npm1): host, column-major, each written when non-NULL; w gets
+ * {W_r, W_t, W_p} when non-NULL.  The B fields go through one transient
+ * device buffer, freed before the call returns. */
+int pot3d_gpu_fields(pot3d_gpu_solver *s, const double *x, double *phi, double *br, double *bt, double *bp,
+                     double w[3]);
+
 /* Kernel-level entry points for parity checks, DEVICE pointers, length N.
  * ax: y = A x as ax (src/pot3d.F90:5102-5150), homogeneous boundaries.
  * prec: x <- M^-1 x as prec_inv (src/pot3d.F90:5152-5225). */

@@ -55,6 +55,7 @@ def lib():
         L.orc_cgsolve.argtypes = [C.c_void_p, dp, dp, C.c_int, C.c_double, C.c_int, ip, dp, ip, ip, dp, C.c_int]
         L.orc_finalize_phi.argtypes = [C.c_void_p, dp, dp]
         L.orc_energy.argtypes = [C.c_void_p, dp, dp]
+        L.orc_getb.argtypes = [C.c_void_p, dp, dp, dp, dp]
         L.orc_get_ai.argtypes = [C.c_void_p, fp]
         L.orc_get_coef.argtypes = [C.c_void_p, dp]
         L.orc_get_ilu_diag.argtypes = [C.c_void_p, fp, fp]
@@ -247,6 +248,16 @@ class Solver:
         w = np.zeros(3)
         lib().orc_energy(self.h, _p(phi), _p(w))
         return w
+
+    def getb(self, phi):
+        """(br, bt, bp) on the staggered meshes (src/pot3d.F90:6187-6233)."""
+        phi = np.asfortranarray(phi, dtype=np.float64)
+        nr, nt, np_ = self.mesh.nr, self.mesh.nt, self.mesh.np
+        br = np.zeros((nr - 1, nt, np_), order="F")
+        bt = np.zeros((nr, nt - 1, np_), order="F")
+        bp = np.zeros((nr, nt, np_ - 1), order="F")
+        lib().orc_getb(self.h, _p(phi), _p(br), _p(bt), _p(bp))
+        return br, bt, bp
 
 
 def ilu0_csr(ia, ja, a):

@@ -1001,6 +1001,33 @@ int orc_energy(orc_ctx *c, const double *phi, double *w) {
   return 0;
 }
 
+/* getb, src/pot3d.F90:6187-6233: B on the staggered meshes, every point the
+ * reference fills.  br is (nrm1,nt,np), bt (nr,ntm1,np), bp (nr,nt,npm1),
+ * column-major; the products in the denominators round left to right. */
+int orc_getb(orc_ctx *c, const double *phi, double *br, double *bt, double *bp) {
+  const int nr = c->nr, nt = c->nt, np = c->np, nrm1 = c->nrm1, ntm1 = c->ntm1, npm1 = c->npm1;
+  const double *dr = c->dr, *rh = c->rh, *dt = c->dt, *sth = c->sth, *dp = c->dp;
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= np; k++)
+    for (int j = 1; j <= nt; j++)
+      for (int i = 1; i <= nrm1; i++)
+        br[(i - 1) + (size_t)nrm1 * ((j - 1) + (size_t)nt * (k - 1))] =
+            (XA(phi, i + 1, j, k) - XA(phi, i, j, k)) / dr[i];
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= np; k++)
+    for (int j = 1; j <= ntm1; j++)
+      for (int i = 1; i <= nr; i++)
+        bt[(i - 1) + (size_t)nr * ((j - 1) + (size_t)ntm1 * (k - 1))] =
+            (XA(phi, i, j + 1, k) - XA(phi, i, j, k)) / (rh[i] * dt[j]);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= npm1; k++)
+    for (int j = 1; j <= nt; j++)
+      for (int i = 1; i <= nr; i++)
+        bp[(i - 1) + (size_t)nr * ((j - 1) + (size_t)nt * (k - 1))] =
+            (XA(phi, i, j, k + 1) - XA(phi, i, j, k)) / (rh[i] * sth[j] * dp[k]);
+  return 0;
+}
+
 int orc_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

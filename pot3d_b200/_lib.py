@@ -18,7 +18,7 @@ MESH_FIELDS = ("r", "dr", "rh", "drh", "t", "dt", "st", "th", "dth", "sth", "p",
 GPU_SYMBOLS = (
     "load_external_lu_solver", "external_lu_solver", "unload_external_lu_solver",
     "pot3d_gpu_create", "pot3d_gpu_destroy", "pot3d_gpu_size", "pot3d_gpu_rhs", "pot3d_gpu_cgsolve",
-    "pot3d_gpu_cgsolve_dev", "pot3d_gpu_history", "pot3d_gpu_finalize_phi", "pot3d_gpu_energy",
+    "pot3d_gpu_cgsolve_dev", "pot3d_gpu_history", "pot3d_gpu_finalize_phi", "pot3d_gpu_energy", "pot3d_gpu_fields",
     "pot3d_gpu_ax_dev", "pot3d_gpu_prec_dev", "pot3d_gpu_precond_diag", "pot3d_gpu_last_error",
     "pot3d_gpu_time_kernels", "pot3d_gpu_time_sweeps", "pot3d_gpu_batch_create", "pot3d_gpu_batch_create_ex", "pot3d_gpu_batch_tune", "pot3d_gpu_batch_solve",
     "pot3d_gpu_batch_solution", "pot3d_gpu_batch_destroy",
@@ -68,6 +68,7 @@ def lib():
         L.pot3d_gpu_history.argtypes = [vp, dp, C.c_int]
         L.pot3d_gpu_finalize_phi.argtypes = [vp, dp, dp]
         L.pot3d_gpu_energy.argtypes = [vp, dp, dp]
+        L.pot3d_gpu_fields.argtypes = [vp, dp, dp, dp, dp, dp, dp]
         L.pot3d_gpu_ax_dev.argtypes = [vp, vp, vp]
         L.pot3d_gpu_prec_dev.argtypes = [vp, vp]
         L.pot3d_gpu_precond_diag.argtypes = [vp, fp, fp]

@@ -168,6 +168,50 @@ extern "C" int pot3d_gpu_energy(pot3d_gpu_solver *h, const double *phi, double w
   return s.energy_dev(s.d_phi, w);
 }
 
+extern "C" int pot3d_gpu_fields(pot3d_gpu_solver *h, const double *x, double *phi, double *br, double *bt,
+                                double *bp, double w[3]) {
+  int st;
+  if ((st = check_solver(h))) return st;
+  if (!x) {
+    pot3d_set_error("pot3d_gpu_fields: null x");
+    return POT3D_ERR_ARG;
+  }
+  Solver &s = h->s;
+  const size_t nr = s.g.nr, nt = s.g.nt, np = s.g.np;
+  const size_t nphi = nr * nt * np;
+  if (!s.d_phi && (st = s.alloc((void **)&s.d_phi, sizeof(double) * nphi))) return st;
+  CKS(cudaMemcpyAsync(h->d_io, x, sizeof(double) * s.g.N, cudaMemcpyHostToDevice, s.stream));
+  if ((st = s.pack(h->d_io, s.d_tmp))) return st;
+  if ((st = s.finalize_phi_dev(s.d_tmp, s.d_phi))) return st;
+  if (phi) CKS(cudaMemcpyAsync(phi, s.d_phi, sizeof(double) * nphi, cudaMemcpyDeviceToHost, s.stream));
+  if (br || bt || bp) {
+    const size_t nbr = (nr - 1) * nt * np, nbt = nr * (nt - 1) * np, nbp = nr * nt * (np - 1);
+    double *d_b = nullptr;
+    if (cudaMallocAsync((void **)&d_b, sizeof(double) * (nbr + nbt + nbp), s.stream) != cudaSuccess) {
+      cudaGetLastError();
+      pot3d_set_error("pot3d_gpu_fields: device allocation of the B fields failed");
+      return POT3D_ERR_NOMEM;
+    }
+    st = s.getb_dev(s.d_phi, d_b, d_b + nbr, d_b + nbr + nbt);
+    if (!st && br)
+      st = pot3d_cuda_status(cudaMemcpyAsync(br, d_b, sizeof(double) * nbr, cudaMemcpyDeviceToHost, s.stream),
+                             "fields: br");
+    if (!st && bt)
+      st = pot3d_cuda_status(
+          cudaMemcpyAsync(bt, d_b + nbr, sizeof(double) * nbt, cudaMemcpyDeviceToHost, s.stream), "fields: bt");
+    if (!st && bp)
+      st = pot3d_cuda_status(
+          cudaMemcpyAsync(bp, d_b + nbr + nbt, sizeof(double) * nbp, cudaMemcpyDeviceToHost, s.stream),
+          "fields: bp");
+    const int fst = pot3d_cuda_status(cudaFreeAsync(d_b, s.stream), "fields: free");
+    if (st) return st;
+    if (fst) return fst;
+  }
+  if (w) return s.energy_dev(s.d_phi, w);
+  CKS(cudaStreamSynchronize(s.stream));
+  return POT3D_OK;
+}
+
 extern "C" int pot3d_gpu_ax_dev(pot3d_gpu_solver *h, const double *x, double *y) {
   int st;
   if ((st = check_solver(h))) return st;

@@ -928,6 +928,28 @@ __global__ void __launch_bounds__(NTHR) k_energy(Geo g, DevMesh m, const double 
     part[3 * blockIdx.x + 2] = s2;
   }
 }
+// getb, src/pot3d.F90:6187-6233: one pass over phi writes every point the
+// reference fills of the three staggered components, br (nrm1,nt,np),
+// bt (nr,ntm1,np) and bp (nr,nt,npm1), column-major.  The denominators'
+// products round left to right, as in the Fortran.
+__global__ void __launch_bounds__(NTHR) k_getb(Geo g, DevMesh m, const double *__restrict__ phi,
+                                               double *__restrict__ br, double *__restrict__ bt,
+                                               double *__restrict__ bp) {
+  const long long nr = g.nr, nt = g.nt, ntr = nr * nt, n = ntr * g.np;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int i0 = (int)(c % nr);
+    const long long jk = c / nr;
+    const int j0 = (int)(jk % nt);
+    const int k0 = (int)(jk / nt);
+    const double f = phi[c];
+    const double rhi = m.rh[i0 + 1];
+    if (i0 < g.nr - 1) br[i0 + (nr - 1) * jk] = (phi[c + 1] - f) / m.dr[i0 + 1];
+    if (j0 < g.nt - 1)
+      bt[i0 + nr * (j0 + (nt - 1) * (long long)k0)] = (phi[c + nr] - f) / __dmul_rn(rhi, m.dt[j0 + 1]);
+    if (k0 < g.np - 1) bp[c] = (phi[c + ntr] - f) / __dmul_rn(__dmul_rn(rhi, m.sth[j0 + 1]), m.dp[k0 + 1]);
+  }
+}
 __global__ void k_energy_final(const double *__restrict__ part, int nb, double *__restrict__ w) {
   if (threadIdx.x < 3) {
     double s = 0.0;
@@ -1617,6 +1639,12 @@ int Solver::finalize_phi_dev(const double *xpad, double *phi) {
   k_phi_poles<<<grid1d((long long)g.nr * (g.np - 2)), NTHR, 0, stream>>>(g, d_sums, phi);
   k_phi_seam<<<grid1d((long long)g.nr * g.nt), NTHR, 0, stream>>>(g, phi);
   return pot3d_cuda_status(cudaGetLastError(), "finalize_phi");
+}
+
+int Solver::getb_dev(const double *phi, double *br, double *bt, double *bp) {
+  const long long n = (long long)g.nr * g.nt * g.np;
+  k_getb<<<grid1d(n), NTHR, 0, stream>>>(g, m, phi, br, bt, bp);
+  return pot3d_cuda_status(cudaGetLastError(), "getb");
 }
 
 int Solver::energy_dev(const double *phi, double w[3]) {

@@ -79,6 +79,8 @@ struct Solver {
   int finalize_phi_dev(const double *xpad, double *phi_dev);
   int time_kernels(int reps, double ms[2], double bytes[2]);
   int sweep_launches() const;  // kernels per ILU(0) application
+  // getb (src/pot3d.F90:6187-6233) from a device phi into device B fields.
+  int getb_dev(const double *phi_dev, double *br, double *bt, double *bp);
   int energy_dev(const double *phi_dev, double w[3]);
 };
 

@@ -137,3 +137,62 @@ def pfss_case(nr, nt, np_, lmax, nbip, seed, option="ss", do_not_balance_flux=Fa
     tn, pn, fi = synthetic_br(seed, lmax, nbip, nt, np_)
     br0 = br0_from_map(mesh, tn, pn, fi, option=option, do_not_balance_flux=do_not_balance_flux)
     return mesh, br0
+
+
+def _seq_sum(a) -> float:
+    """Left-to-right sum (the order of a serial Fortran SUM)."""
+    s = 0.0
+    for v in np.asarray(a, dtype=np.float64).ravel():
+        s += float(v)
+    return s
+
+
+def validation_br(mesh: Mesh, dipole_angle: float, r0: float, r1: float):
+    """set_validation_flux (src/pot3d.F90:3978-4066): the tilted-dipole Br at
+    r0 and r1 on the (nt, np) half mesh, periodic in phi, with the pole ghost
+    rows set from the m=0 average.  Returns (br0, br1), Fortran order."""
+    cth, sth, cph = np.cos(mesh.th), np.sin(mesh.th), np.cos(mesh.ph)
+    ca, sa = np.cos(dipole_angle), np.sin(dipole_angle)
+    pl_i = 1.0 / (2.0 * 3.1415926535897932 - 0.0)
+    nt, np_ = mesh.nt, mesh.np
+    out = []
+    for rr in (r0, r1):
+        b = np.asfortranarray((2.0 / (rr * rr * rr)) * (cth[:, None] * ca + (sth[:, None] * cph[None, :]) * sa))
+        b[:, 0] = b[:, np_ - 2]
+        b[:, np_ - 1] = b[:, 1]
+        s00 = _seq_sum(b[1, 1:np_ - 1] * mesh.dph[1:np_ - 1]) * pl_i
+        s11 = _seq_sum(b[nt - 2, 1:np_ - 1] * mesh.dph[1:np_ - 1]) * pl_i
+        b[0, :] = 2.0 * s00 - b[1, :]
+        b[nt - 1, :] = 2.0 * s11 - b[nt - 2, :]
+        out.append(b)
+    return out[0], out[1]
+
+
+def _seam_phi(a):
+    """seam_gen in the periodic dimension at one rank (src/pot3d.F90:5846-6013)."""
+    n3 = a.shape[2]
+    a[:, :, 0] = a[:, :, n3 - 2]
+    a[:, :, n3 - 1] = a[:, :, 1]
+    return a
+
+
+def validation_exact(mesh: Mesh, dipole_angle: float):
+    """The analytic tilted-dipole solution of write_validation_solution
+    (src/pot3d.F90:4068-4131): phi's interior values (packed, length N; the
+    ghosts follow from the boundary conditions as in the reference) and
+    br (nrm1,nt,np), bt (nr,ntm1,np), bp (nr,nt,npm1) on the staggered
+    meshes, seamed in phi."""
+    ca, sa = np.cos(dipole_angle), np.sin(dipole_angle)
+    nr, nt, np_ = mesh.nr, mesh.nt, mesh.np
+    cth, sth = np.cos(mesh.th), np.sin(mesh.th)
+    ct, st = np.cos(mesh.t), np.sin(mesh.t)
+    cph, sph = np.cos(mesh.ph), np.sin(mesh.ph)
+    ang_h = cth[:, None] * ca + (sth[:, None] * cph[None, :]) * sa          # (nt, np)
+    phi = (-1.0 / (mesh.rh * mesh.rh))[:, None, None] * ang_h[None]
+    x = np.ascontiguousarray(phi[1:-1, 1:-1, 1:-1].transpose(2, 1, 0)).ravel()
+    br = (2.0 / (mesh.r * mesh.r * mesh.r))[:, None, None] * ang_h[None]
+    bt = (1.0 / (mesh.rh * mesh.rh * mesh.rh))[:, None, None] * (st[:, None] * ca - (ct[:, None] * cph[None, :]) * sa)[None]
+    # the reference evaluates bp with the half-mesh sin(ph(k))
+    bp = (1.0 / (mesh.rh * mesh.rh * mesh.rh))[:, None, None] * np.broadcast_to(sph[None, None, :np_ - 1] * sa, (1, nt, np_ - 1))
+    return (x, _seam_phi(np.asfortranarray(br)), _seam_phi(np.asfortranarray(bt)),
+            _seam_phi(np.asfortranarray(bp)))

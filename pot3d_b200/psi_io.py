@@ -246,3 +246,164 @@ def read_psi(path) -> PsiData:
         else:
             scales.append(None)
     return PsiData(data=data, scales=scales, dtype=c_arr.dtype)
+
+
+# ---- writer -------------------------------------------------------------
+#
+# The files POT3D writes (wrhdf_2d/wrhdf_3d, src/psi_io.f90:629-925) hold
+# ``Data`` plus one scale dataset ``dimN`` per axis, each scale marked with
+# the string attribute CLASS = "DIMENSION_SCALE" (h5DSset_scale_f) so that
+# rdh5's h5DSis_scale_f check accepts it, and named with NAME = "dimN".
+# The writer below lays out the same HDF5 subset the reader parses:
+# superblock version 0, one symbol-table root group (a v1 B-tree with one
+# leaf, one local heap, one symbol-table node), version-1 object headers
+# and contiguous, unfiltered little-endian floating-point datasets.  The
+# DIMENSION_LIST / REFERENCE_LIST attributes that the HDF5 library adds
+# when it attaches scales are not written: reading PSI files does not use
+# them (rdh5 matches scales to axes by member order).
+
+_GROUP_LEAF_K = 4
+_GROUP_INTERNAL_K = 16
+_HEAP_FREE_NULL = 1
+
+
+def _pad8(b: bytes) -> bytes:
+    return b + b"\x00" * (-len(b) % 8)
+
+
+def _u(v: int, n: int) -> bytes:
+    return int(v).to_bytes(n, "little")
+
+
+def _msg(mtype: int, body: bytes, flags: int = 0) -> bytes:
+    body = _pad8(body)
+    return _u(mtype, 2) + _u(len(body), 2) + bytes([flags, 0, 0, 0]) + body
+
+
+def _dataspace(shape) -> bytes:
+    # version 1; the maximum dimensions equal the dimensions
+    body = bytes([1, len(shape), 1 if shape else 0, 0]) + _u(0, 4)
+    for d in shape:
+        body += _u(d, 8)
+    for d in shape:
+        body += _u(d, 8)
+    return body
+
+
+def _float_type(itemsize: int) -> bytes:
+    # class 1 (floating point), version 1, little-endian, IEEE layout
+    if itemsize == 8:
+        sign, eloc, esize, msize, bias = 63, 52, 11, 52, 1023
+    else:
+        sign, eloc, esize, msize, bias = 31, 23, 8, 23, 127
+    return (bytes([0x11, 0x20, sign, 0]) + _u(itemsize, 4) + _u(0, 2) + _u(8 * itemsize, 2)
+            + bytes([eloc, esize, 0, msize]) + _u(bias, 4))
+
+
+def _string_attr(name: str, value: str) -> bytes:
+    nm = name.encode("ascii") + b"\x00"
+    val = value.encode("ascii") + b"\x00"
+    dtype = bytes([0x13, 0, 0, 0]) + _u(len(val), 4)  # string, null-terminated, ASCII
+    space = bytes([1, 0, 0, 0]) + _u(0, 4)              # scalar
+    body = (bytes([1, 0]) + _u(len(nm), 2) + _u(len(dtype), 2) + _u(len(space), 2)
+            + _pad8(nm) + _pad8(dtype) + _pad8(space) + val)
+    return _msg(0x000C, body)
+
+
+def _object_header(messages) -> bytes:
+    body = b"".join(messages)
+    return bytes([1, 0]) + _u(len(messages), 2) + _u(1, 4) + _u(len(body), 4) + _u(0, 4) + body
+
+
+def write_psi(path, data, scales=None, hdf32: bool = False) -> None:
+    """Write a PSI HDF5 file readable by ``read_psi`` and by rdh5.
+
+    ``data`` is in Fortran axis order (as ``read_psi`` returns it), 1-3
+    axes; ``scales`` is None or one 1-D array per axis; ``hdf32`` stores
+    FP32 (POT3D's hdf32 option, src/psi_io.f90:629-925), else FP64.
+    """
+    data = np.asarray(data)
+    if not 1 <= data.ndim <= 3:
+        raise ValueError("PSI files hold 1-3 dimensional data")
+    dt = np.dtype("<f4") if hdf32 else np.dtype("<f8")
+    objs = [("Data", np.ascontiguousarray(data.T, dtype=dt), False)]
+    if scales is not None:
+        if len(scales) != data.ndim:
+            raise ValueError("one scale per axis is required")
+        for d, s in enumerate(scales):
+            s = np.ascontiguousarray(np.asarray(s).reshape(-1), dtype=dt)
+            if s.size != data.shape[d]:
+                raise ValueError(f"scale {d + 1} has {s.size} points, axis has {data.shape[d]}")
+            objs.append((f"dim{d + 1}", s, True))
+    objs.sort(key=lambda o: o[0].encode("ascii"))
+
+    # local heap data segment: "" at offset 0, then the names, then one
+    # free block (next = end of list, size 16)
+    heap_names = b"\x00" * 8
+    name_off = {}
+    for name, _, _ in objs:
+        name_off[name] = len(heap_names)
+        heap_names += _pad8(name.encode("ascii") + b"\x00")
+    free_off = len(heap_names)
+    heap_data = heap_names + _u(_HEAP_FREE_NULL, 8) + _u(16, 8)
+
+    root_oh_addr = 96
+    root_oh_size = 16 + 8 + 16
+    btree_addr = root_oh_addr + root_oh_size
+    btree_size = 24 + (2 * _GROUP_INTERNAL_K) * 8 + (2 * _GROUP_INTERNAL_K + 1) * 8
+    heap_addr = btree_addr + btree_size
+    heap_data_addr = heap_addr + 32
+    snod_addr = heap_data_addr + len(heap_data)
+    snod_size = 8 + 2 * _GROUP_LEAF_K * 40
+    if len(objs) > 2 * _GROUP_LEAF_K:
+        raise ValueError("too many datasets for one symbol-table node")
+
+    # object headers (their data addresses are patched in below)
+    def headers(data_addrs):
+        out = []
+        for (name, arr, is_scale), da in zip(objs, data_addrs):
+            msgs = [_msg(0x0001, _dataspace(arr.shape)), _msg(0x0003, _float_type(arr.itemsize), 1),
+                    _msg(0x0005, bytes([2, 2, 2, 1]) + _u(0, 4), 1),
+                    _msg(0x0008, bytes([3, 1]) + _u(da, 8) + _u(arr.nbytes, 8))]
+            if is_scale:
+                msgs += [_string_attr("CLASS", "DIMENSION_SCALE"), _string_attr("NAME", name)]
+            out.append(_object_header(msgs))
+        return out
+
+    hdrs = headers([0] * len(objs))
+    addr = snod_addr + snod_size
+    oh_addrs = []
+    for h in hdrs:
+        oh_addrs.append(addr)
+        addr += len(h)
+    data_addrs = []
+    for _, arr, _ in objs:
+        addr += -addr % 8
+        data_addrs.append(addr)
+        addr += arr.nbytes
+    eof = addr
+    hdrs = headers(data_addrs)
+
+    buf = bytearray(eof)
+    sb = (_SIG + bytes([0, 0, 0, 0, 0, 8, 8, 0]) + _u(_GROUP_LEAF_K, 2) + _u(_GROUP_INTERNAL_K, 2) + _u(0, 4)
+          + _u(0, 8) + _u(_UNDEF, 8) + _u(eof, 8) + _u(_UNDEF, 8))
+    root_entry = _u(0, 8) + _u(root_oh_addr, 8) + _u(1, 4) + _u(0, 4) + _u(btree_addr, 8) + _u(heap_addr, 8)
+    buf[0:96] = sb + root_entry
+    buf[root_oh_addr:root_oh_addr + root_oh_size] = _object_header([_msg(0x0011, _u(btree_addr, 8)
+                                                                         + _u(heap_addr, 8))])
+    tree = (b"TREE" + bytes([0, 0]) + _u(1, 2) + _u(_UNDEF, 8) + _u(_UNDEF, 8)
+            + _u(0, 8) + _u(snod_addr, 8) + _u(name_off[objs[-1][0]], 8))
+    buf[btree_addr:btree_addr + len(tree)] = tree
+    heap = b"HEAP" + bytes([0, 0, 0, 0]) + _u(len(heap_data), 8) + _u(free_off, 8) + _u(heap_data_addr, 8)
+    buf[heap_addr:heap_addr + 32] = heap
+    buf[heap_data_addr:heap_data_addr + len(heap_data)] = heap_data
+    snod = b"SNOD" + bytes([1, 0]) + _u(len(objs), 2)
+    for (name, _, _), oa in zip(objs, oh_addrs):
+        snod += _u(name_off[name], 8) + _u(oa, 8) + _u(0, 4) + _u(0, 4) + b"\x00" * 16
+    buf[snod_addr:snod_addr + len(snod)] = snod
+    for h, oa in zip(hdrs, oh_addrs):
+        buf[oa:oa + len(h)] = h
+    for (_, arr, _), da in zip(objs, data_addrs):
+        buf[da:da + arr.nbytes] = arr.tobytes()
+    with open(path, "wb") as fh:
+        fh.write(bytes(buf))

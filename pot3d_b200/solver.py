@@ -99,6 +99,25 @@ class Pot3dSolver:
         check(_lib.lib().pot3d_gpu_finalize_phi(self._h, dptr(x), dptr(phi)))
         return phi
 
+    def fields(self, x: np.ndarray, want=("phi", "br", "bt", "bp", "w")) -> dict:
+        """phi, B and the magnetic energies from the interior solution x, one
+        device call (potfld's finalisation, getb, magnetic_energy).  Returns
+        the names in ``want``: phi (nr,nt,np), br (nrm1,nt,np),
+        bt (nr,ntm1,np), bp (nr,nt,npm1), Fortran order; w = (W_r, W_t, W_p)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != self.N:
+            raise ValueError(f"x has {x.size} values, the mesh has {self.N} unknowns")
+        nr, nt, np_ = self.mesh.nr, self.mesh.nt, self.mesh.np
+        shapes = {"phi": (nr, nt, np_), "br": (nr - 1, nt, np_), "bt": (nr, nt - 1, np_),
+                  "bp": (nr, nt, np_ - 1), "w": (3,)}
+        unknown = set(want) - set(shapes)
+        if unknown:
+            raise ValueError(f"unknown fields {sorted(unknown)}")
+        out = {k: np.zeros(shapes[k], order="F") for k in want}
+        ptr = [dptr(out[k]) if k in out else None for k in ("phi", "br", "bt", "bp", "w")]
+        check(_lib.lib().pot3d_gpu_fields(self._h, dptr(x), *ptr))
+        return out
+
     def energy(self, phi: np.ndarray) -> np.ndarray:
         phi = np.asfortranarray(phi, dtype=np.float64)
         w = np.zeros(3)

@@ -101,6 +101,31 @@ def test_finalize_and_energy_match_oracle(cuda):
     assert np.all(np.abs(w - w_ref) <= 1e-12 * np.abs(w_ref))
 
 
+@pytest.mark.parametrize("dims", [(37, 30, 26), (20, 13, 11), (9, 7, 8)])
+def test_fields_getb_bitwise(cuda, dims):
+    """phi, br, bt, bp of the one-call post-solve path equal the oracle's
+    getb bit for bit; the energies agree to 1e-12 (summation order)."""
+    mesh, br0 = _case(*dims)
+    s = Pot3dSolver(mesh, br0)
+    o = _oracle(mesh, br0)
+    x = np.random.default_rng(11).standard_normal(s.N)
+    out = s.fields(x)
+    phi_ref = o.finalize_phi(x)
+    assert np.array_equal(out["phi"], phi_ref)
+    for got, ref in zip((out["br"], out["bt"], out["bp"]), o.getb(phi_ref)):
+        assert got.shape == ref.shape
+        assert np.array_equal(got, ref)
+    w_ref = o.energy(phi_ref)
+    assert np.all(np.abs(out["w"] - w_ref) <= 1e-12 * np.abs(w_ref))
+    # subsets: only what is asked for is returned, and it is the same
+    part = s.fields(x, want=("bt", "w"))
+    assert set(part) == {"bt", "w"}
+    assert np.array_equal(part["bt"], out["bt"])
+    assert np.array_equal(part["w"], out["w"])
+    with pytest.raises(ValueError):
+        s.fields(x[:-1])
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_reference_testsuite_energies(cuda, case):
     """The three cases of POT3D's test suite, solved on the GPU: energies

@@ -129,3 +129,27 @@ def test_ncgmax_exceeded_sets_ierr():
     s = O.Solver(m, br0, "ss", 1)
     out = s.cgsolve(np.zeros(s.N), s.rhs(), ncgmax=3, epscg=1e-12)
     assert out["ierr"] == 1 and out["ncg"] == 3
+
+
+def test_getb_restatement_and_energy_consistency():
+    """orc_getb is src/pot3d.F90:6217-6231 (checked bit for bit against a
+    numpy statement of the same formulas), and magnetic_energy, which
+    evaluates B in place, equals the face-averaged energy of getb's fields."""
+    m = O.make_mesh(11, 9, 14)
+    rng = np.random.default_rng(3)
+    s = O.Solver(m, np.zeros((9, 14), order="F"), "ss", 1)
+    phi = s.finalize_phi(rng.standard_normal(s.N))
+    br, bt, bp = s.getb(phi)
+    dr, rh, dt, sth, dp = m.dr, m.rh, m.dt, m.sth, m.dp
+    assert np.array_equal(br, (phi[1:] - phi[:-1]) / dr[:10, None, None])
+    assert np.array_equal(bt, (phi[:, 1:] - phi[:, :-1]) / (rh[:, None, None] * dt[None, :8, None]))
+    den = (rh[:, None] * sth[None, :])[:, :, None] * dp[None, None, :13]
+    assert np.array_equal(bp, (phi[:, :, 1:] - phi[:, :, :-1]) / den)
+    # energy over the interior with face averages (src/pot3d.F90:6279-6292)
+    brav = 0.5 * (br[1:, 1:-1, 1:-1] + br[:-1, 1:-1, 1:-1])
+    btav = 0.5 * (bt[1:-1, 1:, 1:-1] + bt[1:-1, :-1, 1:-1])
+    bpav = 0.5 * (bp[1:-1, 1:-1, 1:] + bp[1:-1, 1:-1, :-1])
+    dv = (rh[1:-1] ** 2 * m.drh[1:-1])[:, None, None] * (m.dth[1:-1] * sth[1:-1])[None, :, None] \
+        * m.dph[None, None, 1:-1]
+    w = [np.sum(0.5 * b * b * dv) for b in (brav, btav, bpav)]
+    assert np.allclose(s.energy(phi), w, rtol=1e-12, atol=0)
