@@ -110,7 +110,8 @@ typedef struct {
  * load_preconditioner_pot3d_solve (src/pot3d.F90:4615-4715).  pm_r1 is the
  * r=R1 switch of check_input (src/pot3d.F90:1250-1285).  br1 may be NULL; if
  * given, the validation-run Neumann condition at r=R1 is used
- * (src/pot3d.F90:5420-5423).  device < 0 means the current device. */
+ * (src/pot3d.F90:5420-5423) and pm_r1 is ignored.  device < 0 means the
+ * current device. */
 int pot3d_gpu_create(const pot3d_mesh_t *mesh, const double *br0, const double *br1,
                      double pm_r1, int ifprec, int precision, int device,
                      pot3d_gpu_solver **out);

@@ -1156,7 +1156,10 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   }
   ifprec = ifprec_;
   precision = precision_;
-  pm_r1 = pm_r1_;
+  // With br1 (a validation run) the r=R1 ghost is x(nr) = x(nrm1) +
+  // vmask*br1*drn (src/pot3d.F90:5420-5423): the operator's homogeneous part
+  // (vmask = 0) couples x(nr) to x(nrm1) with factor +1 whatever the option.
+  pm_r1 = br1 ? 1.0 : pm_r1_;
   g.nr = nr;
   g.nt = nt;
   g.np = np;
