@@ -123,8 +123,10 @@ __global__ void k_dilu_factor(LevelArgs a) {
 // lockstep, one named barrier per step, and exchange them through shared
 // memory.
 //
-// Streams.  One elected thread moves everything a tile reads with the bulk
-// copy engine, a few steps ahead, into rings tracked by mbarriers: the
+// Streams.  A copy warp moves everything a tile reads with the bulk copy
+// engine, a few steps ahead, into rings tracked by mbarriers, refilling a
+// slot as soon as the compute warps report it free, so no copy is issued on
+// their step-to-step dependent path: the
 // sweep's private streams (coefficients and the intermediate y, stored
 // tile-skewed as [tile][group of 4 steps][component][thread] float4 so a
 // group of a block is one contiguous copy) and, forward, the r32 input as
@@ -159,11 +161,13 @@ constexpr int WSK = (WE - 1) + (WJT - 1);
 constexpr int WPG = 11;                 // r32 plane-group slots
 constexpr int WROUT = 32;               // output plane ring (backward z32), > WSK
 constexpr int WXR = 4;                  // exchange ring depth (chunks)
+constexpr int WAVE_BLOCK = WAVE_THREADS + 64;  // + exchange warp + copy warp
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
 constexpr uint32_t WAVE_MBAR_LIMIT = 1u << 26;
 static_assert(WCH % WG == 0, "a chunk is whole stream groups");
 static_assert(WG * WPG > WSK + (WG - 1) + WG * WPD, "a plane group's slot is free when it is reissued");
 static_assert(WROUT > WSK, "a plane is flushed after its last line wrote it");
+static_assert(WPD == WSL - 1, "the r32 plane group of a step group travels with its coefficient group");
 
 struct WaveCtl {
   unsigned ticket, done, epoch;
@@ -210,9 +214,9 @@ struct alignas(128) WaveSmemF {      // forward sweep
   float4 lf[WSL][3][WAVE_THREADS];   // coefficient groups
   float y[2][WJT][WE + 1];           // step parity, line values
   float ring[WXR][2][WCH][16];       // chunk % WXR, face (0: e, 1: j), step in chunk, line
-  uint64_t bar_s[WSL], bar_p[WPG];
+  uint64_t bar_s[WSL];                // one per stream slot, also counting the plane group of the step group
   int2 tile;
-  int abort, ready, consumed, bcase;
+  int abort, ready, consumed, bcase, gdone;
 };
 struct alignas(128) WaveSmemB {      // backward sweep
   float4 ub[WSL][4][WAVE_THREADS];   // coefficient groups
@@ -220,9 +224,9 @@ struct alignas(128) WaveSmemB {      // backward sweep
   float zout[WROUT][WAVE_THREADS];   // z32 planes, slot = plane % WROUT
   float y[2][WJT][WE + 1];
   float ring[WXR][2][WCH][16];
-  uint64_t bar_s[WSL], bar_p[1];
+  uint64_t bar_s[WSL];
   int2 tile;
-  int abort, ready, consumed, bcase;
+  int abort, ready, consumed, bcase, gdone;
 };
 
 template <bool FWD>
@@ -337,8 +341,85 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
   }
 }
 
+// Bounded mbarrier wait of the compute warps that also gives up once the
+// block is aborting (the copy it waits for may then never be issued).
+__device__ __forceinline__ bool wave_mbar_wait(uint64_t *bar, uint32_t parity, const volatile int *abort) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < WAVE_MBAR_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 63) == 63 && *abort) return false;
+  }
+  return false;
+}
+
+// Copy warp: lane 0 issues the tile's bulk copies -- stream group g (the
+// coefficients, backward also the forward's y) and, forward, the r32 plane
+// group g as a TMA box, both completing on the slot's mbarrier -- as soon as
+// the compute warps report the slot free (S.gdone = groups they finished).
+// No copy is issued on the compute warps' dependent path.  Before it
+// returns after an abort, lane 0 waits (bounded) for what it issued.
 template <bool FWD>
-__device__ __forceinline__ bool wave_tile(const WaveArgs &a, const CUtensorMap *rmap,
+__device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *rmap,
+                                          typename WaveSmemSel<FWD>::type &S, const WaveFaces &f, int gbase,
+                                          int qbase, bool acquire_map) {
+  if ((threadIdx.x & 31) != 0) return;
+  const int G = a.nsteps / WG, NQ = (a.g.npm2 + WG - 1) / WG;
+  const int ti = f.ti;
+  const volatile int *abort = &S.abort;
+  if (FWD && acquire_map) tma_acquire_desc(rmap);
+  int ns = 0;
+  unsigned it = 0;
+  while (ns < G && !*abort) {
+    const int gd = *(volatile int *)&S.gdone;
+    __threadfence_block();
+    if (ns < gd + WSL) {
+      // the compute warps' reads of the slots being refilled (ordered before
+      // gdone by their barrier and the fences) precede these async writes
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      do {
+        const int slot = (gbase + ns) % WSL;
+        uint64_t *bar = &S.bar_s[slot];
+        if constexpr (FWD) {
+          const bool plane = ns < NQ;
+          mbar_expect_tx(bar, 3 * WAVE_THREADS * 16 + (plane ? WG * WJT * WE * 4 : 0));
+          bulk_load(&S.lf[slot][0][0], a.lf + ((size_t)ti * G + ns) * 3 * WAVE_THREADS, 3 * WAVE_THREADS * 16,
+                    bar);
+          if (plane)
+            tma_load_3d(&S.rin[(qbase + ns) % WPG][0][0][0], rmap, f.te * WE, f.tj * WJT, ns * WG, bar);
+        } else {
+          mbar_expect_tx(bar, 5 * WAVE_THREADS * 16);
+          bulk_load(&S.ub[slot][0][0], a.ub + ((size_t)ti * G + ns) * 4 * WAVE_THREADS, 4 * WAVE_THREADS * 16,
+                    bar);
+          bulk_load(&S.yin[slot][0], a.ys + ((size_t)ti * G + (G - 1 - ns)) * WAVE_THREADS, WAVE_THREADS * 16,
+                    bar);
+        }
+        ns++;
+      } while (ns < G && ns < gd + WSL);
+      it = 0;
+    } else {
+      if (++it > WAVE_SPIN_LIMIT) {
+        *(volatile int *)&S.abort = 1;
+        break;
+      }
+      __nanosleep(20);
+    }
+  }
+  if (*abort) {  // copies the compute warps may not wait for land before the block moves on
+    for (int g = max(0, ns - WSL); g < ns; g++) {
+      const int gg = gbase + g;
+      mbar_wait(&S.bar_s[gg % WSL], (uint32_t)(gg / WSL) & 1u, WAVE_MBAR_LIMIT);
+    }
+  }
+}
+
+template <bool FWD>
+__device__ __forceinline__ bool wave_tile(const WaveArgs &a,
                                           typename WaveSmemSel<FWD>::type &S, const WaveFaces &f, unsigned epoch,
                                           int gbase, int qbase) {
   const Geo &g = a.g;
@@ -354,7 +435,6 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, const CUtensorMap *
   const int nsteps = a.nsteps;          // a multiple of WCH
   const int shift = FWD ? 0 : a.pad;    // backward: leading idle steps, so its y groups align
   const int G = nsteps / WG;            // stream groups
-  const int NQ = (npm2 + WG - 1) / WG;  // r32 plane groups
   const int te_out = FWD ? te + 1 : te - 1, tj_out = FWD ? tj + 1 : tj - 1;
   const bool pub_e = valid && (FWD ? el == WE - 1 : el == 0) && te_out >= 0 && te_out < a.nte;
   const bool pub_j = valid && (FWD ? jl == WJT - 1 : jl == 0) && tj_out >= 0 && tj_out < a.ntj;
@@ -370,53 +450,13 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, const CUtensorMap *
   const int y_e = ext_e ? 0 : jl * (WE + 1) + (FWD ? el - 1 : el + 1);
   const int y_j = ext_j ? 0 : (FWD ? jl - 1 : jl + 1) * (WE + 1) + el;
 
-  // Thread 0 issues the bulk copies; the mbarrier of a slot counts its uses
-  // over the block's tiles (gbase, qbase) for the wait parity.
-  auto issue_s = [&](int gi) {
-    const int slot = (gbase + gi) % WSL;
-    uint64_t *bar = &S.bar_s[slot];
-    if constexpr (FWD) {
-      mbar_expect_tx(bar, 3 * WAVE_THREADS * 16);
-      bulk_load(&S.lf[slot][0][0], a.lf + ((size_t)ti * G + gi) * 3 * WAVE_THREADS, 3 * WAVE_THREADS * 16, bar);
-    } else {
-      mbar_expect_tx(bar, 5 * WAVE_THREADS * 16);
-      bulk_load(&S.ub[slot][0][0], a.ub + ((size_t)ti * G + gi) * 4 * WAVE_THREADS, 4 * WAVE_THREADS * 16, bar);
-      bulk_load(&S.yin[slot][0], a.ys + ((size_t)ti * G + (G - 1 - gi)) * WAVE_THREADS, WAVE_THREADS * 16, bar);
-    }
-  };
-  auto issue_p = [&](int q) {
-    if constexpr (FWD) {
-      const int slot = (qbase + q) % WPG;
-      mbar_expect_tx(&S.bar_p[slot], WG * WJT * WE * 4);
-      tma_load_3d(&S.rin[slot][0][0][0], rmap, te * WE, tj * WJT, q * WG, &S.bar_p[slot]);
-    }
-  };
+  // The copy warp issues the bulk copies; the mbarrier of a slot counts its
+  // uses over the block's tiles (gbase) for the wait parity.
+  const volatile int *abort = &S.abort;
   auto wait_s = [&](int gi) {
     const int gg = gbase + gi;
-    return mbar_wait(&S.bar_s[gg % WSL], (uint32_t)(gg / WSL) & 1u, WAVE_MBAR_LIMIT);
+    return wave_mbar_wait(&S.bar_s[gg % WSL], (uint32_t)(gg / WSL) & 1u, abort);
   };
-  auto wait_p = [&](int q) {
-    if constexpr (FWD) {
-      const int qq = qbase + q;
-      return mbar_wait(&S.bar_p[qq % WPG], (uint32_t)(qq / WPG) & 1u, WAVE_MBAR_LIMIT);
-    }
-    return true;
-  };
-  // On an abort every copy still in flight lands before the block moves on.
-  int issued_s = 0, issued_p = 0, waited_s = 0, waited_p = 0;
-  auto drain = [&]() {
-    if (T == 0) {
-      for (int gi = waited_s; gi < issued_s; gi++) wait_s(gi);
-      for (int q = waited_p; q < issued_p; q++) wait_p(q);
-    }
-  };
-
-  if (T == 0) {
-    for (int gi = 0; gi < WSL - 1 && gi < G; gi++) issue_s(gi);
-    for (int q = 0; FWD && q < WPD && q < NQ; q++) issue_p(q);
-  }
-  issued_s = min(WSL - 1, G);
-  issued_p = FWD ? min(WPD, NQ) : 0;
 
   // Backward: at step t the plane npm2 + WSK - t is complete (its last line
   // was written at step t-1); each thread stores its own line of it.
@@ -454,31 +494,18 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, const CUtensorMap *
       }
       __threadfence_block();
     }
-    if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) {  // uniform over the compute warps
-      drain();
-      return false;
-    }
+    if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) return false;  // uniform over the compute warps
     const float *ring = &S.ring[c % WXR][0][0][0];
 #pragma unroll
     for (int h = 0; h < WCH / WG; h++) {
       const int gi = c * (WCH / WG) + h;
-      // the slot of group gi-1 was released by the barrier that ended it
+      // the barrier that ended group gi-1 released its slots: tell the copy
+      // warp, which refills them
       if (T == 0) {
-        // the compute warps' reads of the slots being refilled are ordered
-        // (named barrier) before these async-proxy writes
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (gi + WSL - 1 < G) issue_s(gi + WSL - 1);
-        if (FWD && gi + WPD < NQ) issue_p(gi + WPD);
+        __threadfence_block();
+        *(volatile int *)&S.gdone = gi;
       }
-      issued_s = min(gi + WSL, G);
-      if (FWD) issued_p = min(gi + WPD + 1, NQ);
-      bool ok = wait_s(gi);
-      waited_s = gi + 1;
-      if (FWD && gi < NQ) {
-        ok = wait_p(gi) && ok;
-        waited_p = gi + 1;
-      }
-      if (!ok) S.abort = 1;  // acted on at the next chunk
+      if (!wait_s(gi)) S.abort = 1;  // acted on at the next chunk
       const int sl = (gbase + gi) % WSL;
       float4 c0, c1, c2, c3 = make_float4(0.f, 0.f, 0.f, 0.f), yin4 = c3;
       if constexpr (FWD) {
@@ -555,15 +582,14 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a, const CUtensorMap *
 }
 
 template <bool FWD>
-__global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(const __grid_constant__ CUtensorMap rmap,
+__global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_constant__ CUtensorMap rmap,
                                                                     WaveArgs a) {
   using Sm = typename WaveSmemSel<FWD>::type;
   extern __shared__ unsigned char wave_dyn[];
   Sm &S = *reinterpret_cast<Sm *>(wave_dyn + ((128 - (smem_u32(wave_dyn) & 127)) & 127));
-  const bool xwarp = threadIdx.x >= WAVE_THREADS;
+  const int role = threadIdx.x < WAVE_THREADS ? 0 : (threadIdx.x < WAVE_THREADS + 32 ? 1 : 2);  // compute, exchange, copy
   if (threadIdx.x == 0) {
     for (int q = 0; q < WSL; q++) mbar_init(&S.bar_s[q], 1);
-    for (int q = 0; q < (FWD ? WPG : 1); q++) mbar_init(&S.bar_p[q], 1);
     mbar_init_fence();
     if (FWD) tma_prefetch_desc(&rmap);
   }
@@ -579,16 +605,19 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2) k_dilu_wave(const __grid
       S.abort = 0;
       S.ready = 0;
       S.consumed = 0;
+      S.gdone = 0;
     }
     __syncthreads();
     const int2 tile = S.tile;
     if (tile.x < 0) break;
     const WaveFaces f = wave_faces<FWD>(a, tile.x, tile.y);
     bool ok = true;
-    if (xwarp)
+    if (role == 1)
       wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
+    else if (role == 2)
+      wave_copy<FWD>(a, &rmap, S, f, gbase, qbase, false);
     else
-      ok = wave_tile<FWD>(a, &rmap, S, f, epoch, gbase, qbase);
+      ok = wave_tile<FWD>(a, S, f, epoch, gbase, qbase);
     if (!ok) S.abort = 1;
     __syncthreads();
     if (S.abort) {
@@ -626,15 +655,14 @@ struct alignas(64) WaveCase {
 };
 
 template <bool FWD>
-__global__ void __launch_bounds__(WAVE_THREADS + 32, 2)
+__global__ void __launch_bounds__(WAVE_BLOCK, 2)
     k_dilu_wave_batch(const WaveCase *__restrict__ cases, const int4 *__restrict__ order, int total, WaveCtl *ctl) {
   using Sm = typename WaveSmemSel<FWD>::type;
   extern __shared__ unsigned char wave_dyn[];
   Sm &S = *reinterpret_cast<Sm *>(wave_dyn + ((128 - (smem_u32(wave_dyn) & 127)) & 127));
-  const bool xwarp = threadIdx.x >= WAVE_THREADS;
+  const int role = threadIdx.x < WAVE_THREADS ? 0 : (threadIdx.x < WAVE_THREADS + 32 ? 1 : 2);  // compute, exchange, copy
   if (threadIdx.x == 0) {
     for (int q = 0; q < WSL; q++) mbar_init(&S.bar_s[q], 1);
-    for (int q = 0; q < (FWD ? WPG : 1); q++) mbar_init(&S.bar_p[q], 1);
     mbar_init_fence();
   }
   __syncthreads();
@@ -650,13 +678,13 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2)
         const WaveArgs &ca = cases[o.x].a;
         c = (ca.check && *(volatile int *)&ca.st->status != ST_RUNNING) ? -2 : o.x;  // -2: skip
         tl = make_int2(o.y, o.z);
-        if (c >= 0) tma_acquire_desc(&cases[c].rmap);
       }
       S.bcase = c;
       S.tile = tl;
       S.abort = 0;
       S.ready = 0;
       S.consumed = 0;
+      S.gdone = 0;
     }
     __syncthreads();
     const int c = S.bcase;
@@ -670,10 +698,12 @@ __global__ void __launch_bounds__(WAVE_THREADS + 32, 2)
     const WaveArgs &a = C.a;
     const WaveFaces f = wave_faces<FWD>(a, tile.x, tile.y);
     bool ok = true;
-    if (xwarp)
+    if (role == 1)
       wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
+    else if (role == 2)
+      wave_copy<FWD>(a, &C.rmap, S, f, gbase, qbase, true);
     else
-      ok = wave_tile<FWD>(a, &C.rmap, S, f, epoch, gbase, qbase);
+      ok = wave_tile<FWD>(a, S, f, epoch, gbase, qbase);
     if (!ok) S.abort = 1;
     __syncthreads();
     if (S.abort) {
@@ -855,8 +885,8 @@ static int wave_setup(Solver *s) {
   int dev = 0, nsm = 0, occ_f = 0, occ_b = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_THREADS + 32, D->wave_smem_f));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_THREADS + 32, D->wave_smem_b));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_BLOCK, D->wave_smem_f));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_BLOCK, D->wave_smem_b));
   D->wave_blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, D->ntiles));
   return POT3D_OK;
 }
@@ -890,9 +920,9 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   DiluState *D = s->dilu;
   const WaveArgs a = wave_args(s, check);
   if (fwd)
-    k_dilu_wave<true><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_f, s->stream>>>(D->rmap, a);
+    k_dilu_wave<true><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_f, s->stream>>>(D->rmap, a);
   else
-    k_dilu_wave<false><<<D->wave_blocks, WAVE_THREADS + 32, D->wave_smem_b, s->stream>>>(D->rmap, a);
+    k_dilu_wave<false><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_b, s->stream>>>(D->rmap, a);
 }
 
 // ---- batched sweeps over many cases -------------------------------------
@@ -970,10 +1000,10 @@ int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch
       (st = pot3d_cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) ||
       (st = pot3d_cuda_status(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count")) ||
       (st = pot3d_cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave_batch<true>,
-                                                                            WAVE_THREADS + 32, B->smem_f),
+                                                                            WAVE_BLOCK, B->smem_f),
                               "occupancy")) ||
       (st = pot3d_cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave_batch<false>,
-                                                                            WAVE_THREADS + 32, B->smem_b),
+                                                                            WAVE_BLOCK, B->smem_b),
                               "occupancy")))
     return fail(st);
   B->blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, B->total));
@@ -983,9 +1013,9 @@ int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch
 
 // The two sweeps of every running case of the batch (z32 = (LU)^-1 r32).
 int dilu_batch_sweeps(DiluBatch *B, cudaStream_t stream) {
-  k_dilu_wave_batch<true><<<B->blocks, WAVE_THREADS + 32, B->smem_f, stream>>>(B->d_cases, B->d_order, B->total,
+  k_dilu_wave_batch<true><<<B->blocks, WAVE_BLOCK, B->smem_f, stream>>>(B->d_cases, B->d_order, B->total,
                                                                               B->ctl);
-  k_dilu_wave_batch<false><<<B->blocks, WAVE_THREADS + 32, B->smem_b, stream>>>(B->d_cases, B->d_order, B->total,
+  k_dilu_wave_batch<false><<<B->blocks, WAVE_BLOCK, B->smem_b, stream>>>(B->d_cases, B->d_order, B->total,
                                                                                B->ctl);
   return pot3d_cuda_status(cudaGetLastError(), "batched ILU(0) sweeps");
 }
