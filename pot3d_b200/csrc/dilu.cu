@@ -281,15 +281,6 @@ __device__ __forceinline__ bool wave_needed(const WaveArgs &a, const WaveFaces &
   const int q = t - (FWD ? 0 : a.pad) - sk_c;
   return t < a.ndiag && q >= 0 && q < a.g.npm2;
 }
-__device__ __forceinline__ bool wave_spin(const unsigned long long *p, unsigned epoch, unsigned long long *w) {
-  unsigned it = 0;
-  while ((unsigned)(*w >> 32) != epoch) {
-    if (++it > WAVE_SPIN_LIMIT) return false;
-    if (it > 8) __nanosleep(32);
-    *w = wave_load(p);
-  }
-  return true;
-}
 
 // Exchange warp: fills the face ring WXR chunks ahead of the compute warps.
 // Lane L serves face L >> 4, line L & 15, all WCH steps of a chunk.
@@ -312,25 +303,34 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
     if (*(volatile int *)&S.abort) return;
     bool ok = true;
     unsigned long long w[WCH];
-    // the chunk's last needed word of this line first: once it is current
-    // the earlier ones (published earlier by the same producer thread) are
-    // almost always visible too
+    // every needed word of the chunk is loaded in each poll round (the loads
+    // overlap), and a round reloads only the words not yet current
     int last = -1;
 #pragma unroll
     for (int s = 0; s < WCH; s++)
       if (wave_needed<FWD>(a, f, face, line, c * WCH + s)) last = s;
+    const unsigned long long done_word = (unsigned long long)epoch << 32;
+#pragma unroll
+    for (int s = 0; s < WCH; s++)
+      w[s] = (s <= last && wave_needed<FWD>(a, f, face, line, c * WCH + s)) ? 0ull : done_word;
     if (last >= 0) {
-      unsigned long long wl = wave_load(src + (size_t)(c * WCH + last) * 16);
-      ok = wave_spin(src + (size_t)(c * WCH + last) * 16, epoch, &wl);
+      unsigned it = 0;
+      for (;;) {
 #pragma unroll
-      for (int s = 0; s < WCH; s++)
-        w[s] = (s <= last && wave_needed<FWD>(a, f, face, line, c * WCH + s)) ? wave_load(src + (size_t)(c * WCH + s) * 16)
-                                                                                : ((unsigned long long)epoch << 32);
+        for (int s = 0; s < WCH; s++)
+          if ((unsigned)(w[s] >> 32) != epoch) w[s] = wave_load(src + (size_t)(c * WCH + s) * 16);
+        bool cur = true;
 #pragma unroll
-      for (int s = 0; s < WCH; s++) {
-        ok = ok && wave_spin(src + (size_t)(c * WCH + s) * 16, epoch, &w[s]);
-        S.ring[c % WXR][face][s][line] = __uint_as_float((unsigned)w[s]);
+        for (int s = 0; s < WCH; s++) cur = cur && (unsigned)(w[s] >> 32) == epoch;
+        if (cur) break;
+        if (++it > WAVE_SPIN_LIMIT) {
+          ok = false;
+          break;
+        }
+        if (it > 8) __nanosleep(32);
       }
+#pragma unroll
+      for (int s = 0; s < WCH; s++) S.ring[c % WXR][face][s][line] = __uint_as_float((unsigned)w[s]);
     }
     if (!ok) S.abort = 1;
     __syncwarp();
