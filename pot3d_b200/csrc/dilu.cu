@@ -282,7 +282,8 @@ __device__ __forceinline__ bool wave_needed(const WaveArgs &a, const WaveFaces &
   return t < a.ndiag && q >= 0 && q < a.g.npm2;
 }
 
-// Exchange warp: fills the face ring WXR chunks ahead of the compute warps.
+// Exchange warp: fills the face ring WXR chunks ahead of the compute warps,
+// handing each 4-step group of a chunk over as soon as its words are current.
 // Lane L serves face L >> 4, line L & 15, all WCH steps of a chunk.
 template <bool FWD>
 __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSmemSel<FWD>::type &S,
@@ -300,44 +301,49 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
       }
       __nanosleep(64);
     }
-    if (*(volatile int *)&S.abort) return;
+    if (__any_sync(0xffffffffu, *(volatile int *)&S.abort != 0)) return;  // uniform over the warp
     bool ok = true;
     unsigned long long w[WCH];
     // every needed word of the chunk is loaded in each poll round (the loads
-    // overlap), and a round reloads only the words not yet current
-    int last = -1;
-#pragma unroll
-    for (int s = 0; s < WCH; s++)
-      if (wave_needed<FWD>(a, f, face, line, c * WCH + s)) last = s;
+    // overlap), and a round reloads only the words not yet current; each
+    // step group of the chunk is handed to the compute warps (S.ready counts
+    // groups) as soon as all its words are current
     const unsigned long long done_word = (unsigned long long)epoch << 32;
 #pragma unroll
     for (int s = 0; s < WCH; s++)
-      w[s] = (s <= last && wave_needed<FWD>(a, f, face, line, c * WCH + s)) ? 0ull : done_word;
-    if (last >= 0) {
-      unsigned it = 0;
-      for (;;) {
+      w[s] = wave_needed<FWD>(a, f, face, line, c * WCH + s) ? 0ull : done_word;
+    constexpr int NGC = WCH / WG;  // step groups per chunk
+    int pub = 0;                   // groups of this chunk handed over
+    unsigned pit = 0;
+    for (;;) {
 #pragma unroll
-        for (int s = 0; s < WCH; s++)
-          if ((unsigned)(w[s] >> 32) != epoch) w[s] = wave_load(src + (size_t)(c * WCH + s) * 16);
+      for (int s = 0; s < WCH; s++)
+        if ((unsigned)(w[s] >> 32) != epoch) w[s] = wave_load(src + (size_t)(c * WCH + s) * 16);
+      while (pub < NGC) {
         bool cur = true;
 #pragma unroll
-        for (int s = 0; s < WCH; s++) cur = cur && (unsigned)(w[s] >> 32) == epoch;
-        if (cur) break;
-        if (++it > WAVE_SPIN_LIMIT) {
-          ok = false;
-          break;
-        }
-        if (it > 8) __nanosleep(32);
-      }
+        for (int s = 0; s < WCH; s++)
+          if (s / WG == pub) cur = cur && (unsigned)(w[s] >> 32) == epoch;
+        if (!__all_sync(0xffffffffu, cur)) break;
 #pragma unroll
-      for (int s = 0; s < WCH; s++) S.ring[c % WXR][face][s][line] = __uint_as_float((unsigned)w[s]);
+        for (int s = 0; s < WCH; s++)
+          if (s / WG == pub) S.ring[c % WXR][face][s][line] = __uint_as_float((unsigned)w[s]);
+        __syncwarp();
+        pub++;
+        if (lane == 0) {
+          __threadfence_block();
+          *(volatile int *)&S.ready = c * NGC + pub;
+        }
+      }
+      if (pub == NGC) break;
+      if (++pit > WAVE_SPIN_LIMIT) {
+        ok = false;
+        break;
+      }
+      if (pit > 8) __nanosleep(32);
     }
     if (!ok) S.abort = 1;
     __syncwarp();
-    if (lane == 0) {
-      __threadfence_block();
-      *(volatile int *)&S.ready = c + 1;
-    }
   }
 }
 
@@ -483,22 +489,22 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
   }
 #pragma unroll 1
   for (int c = 0; c < nch; c++) {
-    {  // wait until the exchange warp has chunk c in the ring
-      unsigned it = 0;
-      while (*(volatile int *)&S.ready <= c && !*(volatile int *)&S.abort) {
-        if (++it > WAVE_SPIN_LIMIT) {
-          S.abort = 1;
-          break;
-        }
-        if (it > 4) __nanosleep(32);
-      }
-      __threadfence_block();
-    }
-    if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) return false;  // uniform over the compute warps
     const float *ring = &S.ring[c % WXR][0][0][0];
 #pragma unroll
     for (int h = 0; h < WCH / WG; h++) {
       const int gi = c * (WCH / WG) + h;
+      {  // wait until the exchange warp has step group gi in the ring
+        unsigned it = 0;
+        while (*(volatile int *)&S.ready <= gi && !*(volatile int *)&S.abort) {
+          if (++it > WAVE_SPIN_LIMIT) {
+            S.abort = 1;
+            break;
+          }
+          if (it > 4) __nanosleep(32);
+        }
+        __threadfence_block();
+      }
+      if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) return false;  // uniform over the compute warps
       // the barrier that ended group gi-1 released its slots: tell the copy
       // warp, which refills them
       if (T == 0) {
