@@ -482,8 +482,11 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
   }
 }
 
+// The PCGZ stages (one FP64 and one FP32 box per plane) fit three blocks per
+// SM in shared memory, so that mode is compiled for three; the others hold
+// more per stage and stay at two (a tighter register cap only slows them).
 template <int MODE>
-__global__ void __launch_bounds__(NTHR, 2)
+__global__ void __launch_bounds__(NTHR, MODE == MODE_PCGZ ? 3 : 2)
     k_stencil(const __grid_constant__ StencilMaps maps, Geo g, DevMesh m, StencilArgs a) {
   stencil_body<MODE>(maps, g, m, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
