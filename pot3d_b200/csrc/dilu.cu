@@ -132,9 +132,10 @@ __global__ void k_dilu_factor(LevelArgs a) {
 // group of a block is one contiguous copy) and, forward, the r32 input as
 // 16 x 16 x 4 boxes of phi planes (a 3-D TMA load, no multicast).  A thread
 // then reads 4 steps of a coefficient with one 128-bit shared load.  The
-// backward sweep's z32 output goes through a ring of phi planes: every
-// thread stores its own line of the plane completed at the previous step,
-// so each warp writes two 64-byte row segments.
+// backward sweep's z32 output goes through a 40-plane ring in shared
+// memory: each finished plane of the tile leaves as one 16 x 16 TMA store
+// issued by the copy warp, which hands the slot back once the store has read
+// it, so the compute warps issue no global stores for z32.
 //
 // Across tile faces values travel as 64-bit words holding the FP32 value
 // and a sweep tag, indexed by the step at which the consumer needs them, so
@@ -159,14 +160,14 @@ constexpr int WSL = 3;                  // stream group slots (groups g+1, g+2 i
 constexpr int WPD = 2;                  // r32 plane groups issued ahead
 constexpr int WSK = (WE - 1) + (WJT - 1);
 constexpr int WPG = 11;                 // r32 plane-group slots
-constexpr int WROUT = 32;               // output plane ring (backward z32), > WSK
+constexpr int WROUT = 40;               // output plane ring (backward z32)
 constexpr int WXR = 4;                  // exchange ring depth (chunks)
 constexpr int WAVE_BLOCK = WAVE_THREADS + 64;  // + exchange warp + copy warp
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
 constexpr uint32_t WAVE_MBAR_LIMIT = 1u << 26;
 static_assert(WCH % WG == 0, "a chunk is whole stream groups");
 static_assert(WG * WPG > WSK + (WG - 1) + WG * WPD, "a plane group's slot is free when it is reissued");
-static_assert(WROUT > WSK, "a plane is flushed after its last line wrote it");
+static_assert(WROUT >= WSK + 2 * WG + 2, "the copy warp stores a finished plane before its slot is needed again");
 static_assert(WPD == WSL - 1, "the r32 plane group of a step group travels with its coefficient group");
 
 struct WaveCtl {
@@ -216,17 +217,17 @@ struct alignas(128) WaveSmemF {      // forward sweep
   float ring[WXR][2][WCH][16];       // chunk % WXR, face (0: e, 1: j), step in chunk, line
   uint64_t bar_s[WSL];                // one per stream slot, also counting the plane group of the step group
   int2 tile;
-  int abort, ready, consumed, bcase, gdone;
+  int abort, ready, consumed, bcase, gdone, zflushed;
 };
 struct alignas(128) WaveSmemB {      // backward sweep
   float4 ub[WSL][4][WAVE_THREADS];   // coefficient groups
   float4 yin[WSL][WAVE_THREADS];     // y groups
-  float zout[WROUT][WAVE_THREADS];   // z32 planes, slot = plane % WROUT
+  float zout[WROUT][WAVE_THREADS];   // z32 planes [jl][el], slot = plane % WROUT (TMA store source)
   float y[2][WJT][WE + 1];
   float ring[WXR][2][WCH][16];
   uint64_t bar_s[WSL];
   int2 tile;
-  int abort, ready, consumed, bcase, gdone;
+  int abort, ready, consumed, bcase, gdone, zflushed;
 };
 
 template <bool FWD>
@@ -371,20 +372,24 @@ __device__ __forceinline__ bool wave_mbar_wait(uint64_t *bar, uint32_t parity, c
 // No copy is issued on the compute warps' dependent path.  Before it
 // returns after an abort, lane 0 waits (bounded) for what it issued.
 template <bool FWD>
-__device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *rmap,
+__device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *map,
                                           typename WaveSmemSel<FWD>::type &S, const WaveFaces &f, int gbase,
                                           int qbase, bool acquire_map) {
   if ((threadIdx.x & 31) != 0) return;
   const int G = a.nsteps / WG, NQ = (a.g.npm2 + WG - 1) / WG;
+  const int npm2 = a.g.npm2;
+  const int shift = FWD ? 0 : a.pad;
   const int ti = f.ti;
   const volatile int *abort = &S.abort;
-  if (FWD && acquire_map) tma_acquire_desc(rmap);
+  if (acquire_map) tma_acquire_desc(map);
   int ns = 0;
+  int zd = 0;  // backward: z32 planes stored, from the top (npm2-1, npm2-2, ...)
   unsigned it = 0;
-  while (ns < G && !*abort) {
+  while ((ns < G || (!FWD && zd < npm2)) && !*abort) {
     const int gd = *(volatile int *)&S.gdone;
     __threadfence_block();
-    if (ns < gd + WSL) {
+    bool worked = false;
+    if (ns < G && ns < gd + WSL) {
       // the compute warps' reads of the slots being refilled (ordered before
       // gdone by their barrier and the fences) precede these async writes
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -397,7 +402,7 @@ __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *
           bulk_load(&S.lf[slot][0][0], a.lf + ((size_t)ti * G + ns) * 3 * WAVE_THREADS, 3 * WAVE_THREADS * 16,
                     bar);
           if (plane)
-            tma_load_3d(&S.rin[(qbase + ns) % WPG][0][0][0], rmap, f.te * WE, f.tj * WJT, ns * WG, bar);
+            tma_load_3d(&S.rin[(qbase + ns) % WPG][0][0][0], map, f.te * WE, f.tj * WJT, ns * WG, bar);
         } else {
           mbar_expect_tx(bar, 5 * WAVE_THREADS * 16);
           bulk_load(&S.ub[slot][0][0], a.ub + ((size_t)ti * G + ns) * 4 * WAVE_THREADS, 4 * WAVE_THREADS * 16,
@@ -407,6 +412,29 @@ __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *
         }
         ns++;
       } while (ns < G && ns < gd + WSL);
+      worked = true;
+    }
+    if constexpr (!FWD) {
+      // Plane kd is finished once step npm2 + WSK + shift - kd - 1 is over:
+      // with gd groups done, the top 4 gd - WSK - shift planes are.  Each is
+      // stored from its ring slot as one 16 x 16 box (clipped at the
+      // interior's edges); the slot is handed back (zflushed) once the store
+      // has read it.
+      const int nc = min(npm2, max(0, WG * gd - WSK - shift));
+      if (zd < nc) {
+        do {
+          const int kd = npm2 - 1 - zd;
+          tma_store_3d(map, f.te * WE, f.tj * WJT, kd, &S.zout[kd % WROUT][0]);
+          zd++;
+        } while (zd < nc);
+        bulk_commit();
+        bulk_wait_read_all();
+        __threadfence_block();
+        *(volatile int *)&S.zflushed = zd;
+        worked = true;
+      }
+    }
+    if (worked) {
       it = 0;
     } else {
       if (++it > WAVE_SPIN_LIMIT) {
@@ -422,6 +450,7 @@ __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *
       mbar_wait(&S.bar_s[gg % WSL], (uint32_t)(gg / WSL) & 1u, WAVE_MBAR_LIMIT);
     }
   }
+  if constexpr (!FWD) bulk_wait_all();  // the tile's z32 planes are in global memory
 }
 
 template <bool FWD>
@@ -436,7 +465,6 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
   const bool valid = e < g.nrm2 && jj < g.ntm2;
   const int sk = FWD ? el + jl : (WE - 1 - el) + (WJT - 1 - jl);
   const int npm2 = g.npm2;
-  const long long plane = (long long)g.ntm2 * g.NRP;
   const long long row = (long long)(valid ? jj : 0) * g.NRP + (valid ? e : 0);
   const int nsteps = a.nsteps;          // a multiple of WCH
   const int shift = FWD ? 0 : a.pad;    // backward: leading idle steps, so its y groups align
@@ -462,18 +490,6 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
   auto wait_s = [&](int gi) {
     const int gg = gbase + gi;
     return wave_mbar_wait(&S.bar_s[gg % WSL], (uint32_t)(gg / WSL) & 1u, abort);
-  };
-
-  // Backward: at step t the plane npm2 + WSK - t is complete (its last line
-  // was written at step t-1); each thread stores its own line of it.
-  int flushed_to = -1;  // last step whose plane was flushed
-  auto flush = [&](int t) {
-    if constexpr (!FWD) {
-      const int kd = npm2 + WSK + shift - t;
-      if (kd < 0 || kd >= npm2 || t - shift <= WSK) return;
-      flushed_to = t;
-      if (valid) a.z32[(long long)kd * plane + row] = S.zout[kd % WROUT][T];
-    }
   };
 
   float seam_y = 0.f;  // value at the line's first plane of the sweep
@@ -512,6 +528,20 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         *(volatile int *)&S.gdone = gi;
       }
       if (!wait_s(gi)) S.abort = 1;  // acted on at the next chunk
+      if constexpr (!FWD) {
+        // this group writes planes down to npm2 - WG (gi + 1) + shift; the
+        // slot of each held the plane WROUT above it, which the copy warp
+        // must have stored first
+        const int need = WG * gi + WG - shift - WROUT;
+        unsigned it = 0;
+        while (*(volatile int *)&S.zflushed < need && !*(volatile int *)&S.abort) {
+          if (++it > WAVE_SPIN_LIMIT) {
+            S.abort = 1;
+            break;
+          }
+          __nanosleep(20);
+        }
+      }
       const int sl = (gbase + gi) % WSL;
       float4 c0, c1, c2, c3 = make_float4(0.f, 0.f, 0.f, 0.f), yin4 = c3;
       if constexpr (FWD) {
@@ -531,7 +561,6 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         const int t = gi * WG + u;
         const int uc = h * WG + u;  // step within the chunk
         const float *yprev = &S.y[(t + 1) & 1][0][0];  // values of step t-1
-        if constexpr (!FWD) flush(t);
         const float k0 = u == 0 ? c0.x : u == 1 ? c0.y : u == 2 ? c0.z : c0.w;
         const float k1 = u == 0 ? c1.x : u == 1 ? c1.y : u == 2 ? c1.z : c1.w;
         const float k2 = u == 0 ? c2.x : u == 1 ? c2.y : u == 2 ? c2.z : c2.w;
@@ -575,20 +604,25 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
           prev = y;
         }
         y4[u] = y;
+        // backward: the group's z32 plane writes become visible to the copy
+        // warp's TMA stores (async proxy) across the barrier and gdone
+        if (!FWD && u == WG - 1) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         wave_bar_compute();
       }
       if constexpr (FWD) a.ys[((size_t)ti * G + gi) * WAVE_THREADS + T] = make_float4(y4[0], y4[1], y4[2], y4[3]);
     }
     if (T == 0) *(volatile int *)&S.consumed = c + 1;
   }
-  if constexpr (!FWD) {  // the first plane completes at step npm2 + WSK + shift
-    if (flushed_to < npm2 + WSK + shift) flush(npm2 + WSK + shift);
+  if (T == 0) {  // every group is done: the copy warp stores the last planes
+    __threadfence_block();
+    *(volatile int *)&S.gdone = G;
   }
   return true;
 }
 
 template <bool FWD>
-__global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_constant__ CUtensorMap rmap,
+// map: forward, the r32 load map; backward, the z32 store map.
+__global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_constant__ CUtensorMap map,
                                                                     WaveArgs a) {
   using Sm = typename WaveSmemSel<FWD>::type;
   extern __shared__ unsigned char wave_dyn[];
@@ -597,7 +631,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
   if (threadIdx.x == 0) {
     for (int q = 0; q < WSL; q++) mbar_init(&S.bar_s[q], 1);
     mbar_init_fence();
-    if (FWD) tma_prefetch_desc(&rmap);
+    tma_prefetch_desc(&map);
   }
   __syncthreads();
   const unsigned epoch = *(volatile unsigned *)&a.ctl->epoch;
@@ -612,6 +646,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
       S.ready = 0;
       S.consumed = 0;
       S.gdone = 0;
+      S.zflushed = 0;
     }
     __syncthreads();
     const int2 tile = S.tile;
@@ -621,7 +656,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
     if (role == 1)
       wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
     else if (role == 2)
-      wave_copy<FWD>(a, &rmap, S, f, gbase, qbase, false);
+      wave_copy<FWD>(a, &map, S, f, gbase, qbase, false);
     else
       ok = wave_tile<FWD>(a, S, f, epoch, gbase, qbase);
     if (!ok) S.abort = 1;
@@ -656,7 +691,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
 // the map acquired for the tensormap proxy since it reached global memory by
 // a host copy); tiles of a case that is no longer running are skipped.
 struct alignas(64) WaveCase {
-  CUtensorMap rmap;
+  CUtensorMap rmap;  // forward: r32 loads
+  CUtensorMap zmap;  // backward: z32 stores
   WaveArgs a;
 };
 
@@ -691,6 +727,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2)
       S.ready = 0;
       S.consumed = 0;
       S.gdone = 0;
+      S.zflushed = 0;
     }
     __syncthreads();
     const int c = S.bcase;
@@ -707,7 +744,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2)
     if (role == 1)
       wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
     else if (role == 2)
-      wave_copy<FWD>(a, &C.rmap, S, f, gbase, qbase, true);
+      wave_copy<FWD>(a, FWD ? &C.rmap : &C.zmap, S, f, gbase, qbase, true);
     else
       ok = wave_tile<FWD>(a, S, f, epoch, gbase, qbase);
     if (!ok) S.abort = 1;
@@ -817,7 +854,8 @@ struct DiluState {
   float *seam_f = nullptr, *seam_b = nullptr;
   int2 *order = nullptr;
   WaveCtl *ctl = nullptr;
-  CUtensorMap rmap;  // r32 in 16 x 16 x 4 boxes
+  CUtensorMap rmap;  // r32 in 16 x 16 x 4 boxes (forward loads)
+  CUtensorMap zmap;  // z32 interior in 16 x 16 x 1 boxes (backward stores)
   int nte = 0, ntj = 0, ntiles = 0, ndiag = 0, nsteps = 0, wave_blocks = 0;
   size_t wave_smem_f = 0, wave_smem_b = 0;
 };
@@ -866,6 +904,7 @@ static int wave_setup(Solver *s) {
       (st = s->alloc((void **)&D->ctl, sizeof(WaveCtl))))
     return st;
   if ((st = encode_padded_map(g, D->r32, false, WE, WJT, WG, &D->rmap))) return st;
+  if ((st = encode_padded_map(g, D->z32, false, WE, WJT, 1, &D->zmap, true))) return st;
   // Tickets in order of the tile's first wavefront step WE te + WJT tj
   // (ties by te): a tile's producers (te-1, tj) and (te, tj-1) have smaller
   // keys; the backward sweep takes the tickets in reverse.
@@ -928,7 +967,7 @@ static void launch_wave(Solver *s, bool fwd, bool check) {
   if (fwd)
     k_dilu_wave<true><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_f, s->stream>>>(D->rmap, a);
   else
-    k_dilu_wave<false><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_b, s->stream>>>(D->rmap, a);
+    k_dilu_wave<false><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_b, s->stream>>>(D->zmap, a);
 }
 
 // ---- batched sweeps over many cases -------------------------------------
@@ -961,6 +1000,7 @@ int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch
       return POT3D_ERR_ARG;
     }
     h[q].rmap = D->rmap;
+    h[q].zmap = D->zmap;
     h[q].a = wave_args(cases[q], true);
     for (int tj = 0; tj < D->ntj; tj++)
       for (int te = 0; te < D->nte; te++) ord.push_back(make_int4(q, te, tj, 0));

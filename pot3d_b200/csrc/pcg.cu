@@ -1039,14 +1039,17 @@ static EncodeTiledFn encode_tiled() {
 
 // 3-D tensor map of a padded vector (i, j, k) = (NRP, ntm2, npm2) with a
 // box of bx x by x bz elements; zero fill outside the vector.
-int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, int bz, CUtensorMap *out) {
+int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, int bz, CUtensorMap *out,
+                      bool interior_only) {
   EncodeTiledFn fn = encode_tiled();
   if (!fn) {
     pot3d_set_error("cuTensorMapEncodeTiled is not available from the driver");
     return POT3D_ERR_CUDA;
   }
   const cuuint64_t es = fp64 ? 8 : 4;
-  cuuint64_t dims[3] = {(cuuint64_t)g.NRP, (cuuint64_t)g.ntm2, (cuuint64_t)g.npm2};
+  // interior_only: the map ends at e = nrm2, so a store through it never
+  // writes the padding columns of a line
+  cuuint64_t dims[3] = {(cuuint64_t)(interior_only ? g.nrm2 : g.NRP), (cuuint64_t)g.ntm2, (cuuint64_t)g.npm2};
   cuuint64_t strides[2] = {(cuuint64_t)g.NRP * es, (cuuint64_t)g.NRP * g.ntm2 * es};
   cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
   cuuint32_t estr[3] = {1, 1, 1};

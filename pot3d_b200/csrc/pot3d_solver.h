@@ -92,7 +92,8 @@ float *dilu_z32(Solver *s);   // FP32 output z = (LU)^-1 r32
 // Forward + backward sweeps r32 -> z32 on s->stream; with check_status the
 // kernels return at once when the PCG state is no longer running.
 int dilu_sweeps(Solver *s, bool check_status);
-int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, int bz, CUtensorMap *out);
+int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, int bz, CUtensorMap *out,
+                      bool interior_only = false);
 int dilu_reset(Solver *s);
 int dilu_status(Solver *s);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
 int dilu_time(Solver *s, int reps, double ms[2]);
