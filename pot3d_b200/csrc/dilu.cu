@@ -217,7 +217,7 @@ struct alignas(128) WaveSmemF {      // forward sweep
   float ring[WXR][2][WCH][16];       // chunk % WXR, face (0: e, 1: j), step in chunk, line
   uint64_t bar_s[WSL];                // one per stream slot, also counting the plane group of the step group
   int2 tile;
-  int abort, ready, consumed, bcase, gdone, zflushed;
+  int abort, ready, consumed, bcase, gdone, zflushed;  // zflushed unused forward
 };
 struct alignas(128) WaveSmemB {      // backward sweep
   float4 ub[WSL][4][WAVE_THREADS];   // coefficient groups
@@ -227,6 +227,7 @@ struct alignas(128) WaveSmemB {      // backward sweep
   float ring[WXR][2][WCH][16];
   uint64_t bar_s[WSL];
   int2 tile;
+  // zflushed: z32 planes, from the top, whose TMA store has read its slot
   int abort, ready, consumed, bcase, gdone, zflushed;
 };
 
