@@ -15,8 +15,8 @@ beside it (`plain_fp64`).
 
 value: device time of the solve (CUDA events on the library's stream around
 the PCG initialisation and iterations), inputs resident in HBM.
-e2e: the same solve through the C-ABI with host buffers, pot3d_gpu_cgsolve,
-host<->device copies of x and r included, wall time.
+e2e: the same solve through the C-ABI with pinned host buffers,
+pot3d_gpu_cgsolve, host<->device copies of x and r included, wall time.
 The working set (~2.6 GB of vectors, plus ~2.5 GB of sweep coefficient
 streams with ILU(0)) is 20x the 126 MB L2, so no flush is needed between
 steps.
@@ -342,10 +342,12 @@ def main():
     barrier(ws)
     t_dev = reduce_max(float(np.mean(dev_times)), ws)
 
-    # End to end through the host-pointer C-ABI (H2D + solve + D2H); with the
-    # learned guess also the map's upload and the guess's download.
-    x_h = np.zeros(N)
-    r_h = np.empty(N)
+    # End to end through the host-pointer C-ABI (H2D + solve + D2H) on pinned
+    # host buffers; with the learned guess also the map's upload and the
+    # guess's download.
+    x_pin = torch.zeros(N, dtype=torch.float64, pin_memory=True)
+    r_pin = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    x_h, r_h = x_pin.numpy(), r_pin.numpy()
     e2e = []
     h2d, d2h = 16 * N, 16 * N
     for it in range(args.steps):
@@ -355,7 +357,7 @@ def main():
         if model is not None:
             br0n_d.copy_(br0n_h)
             guess_into(xt)
-            x_h[:] = xt.cpu().numpy()
+            x_pin.copy_(xt)
         else:
             x_h[:] = 0.0
         s.cgsolve(x_h, r_h, epscg=args.epscg)
