@@ -40,9 +40,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "solve s to 1e-9 resid: learned+FP32-refined vs plain FP64 PCG on 1 B200; HBM GB/s"
-# Iteration counts of the seeded workloads' GPU solves (FP64 PCG to 1e-9),
-# used to project the reference arm's CPU sample to a whole solve.
-SOLVE_ITERATIONS = {("pfss_255x361x721", 1): 7036, ("pfss_255x361x721", 2): 1094}
+# Iteration counts of the seeded workloads' solves from a zero guess (FP64
+# PCG to 1e-9; (workload, ifprec) -> iterations), used to project the
+# reference arm's CPU sample to a whole solve: the GPU solves' counts, and
+# for the two smaller grids the oracle's full solves.
+SOLVE_ITERATIONS = {("pfss_255x361x721", 1): 7036, ("pfss_255x361x721", 2): 1094,
+                    ("pfss_63x91x181", 1): 1302, ("pfss_63x91x181", 2): 273,
+                    ("pfss_127x181x361", 1): 3064,
+                    ("open_511x721x1441", 1): 15639, ("open_511x721x1441", 2): 2165}
 # Algorithmic DRAM bytes per unknown and PCG iteration: diagonal
 # preconditioner 80 (stencil r, p -> p, Ap; update x, p, r, Ap -> x, r);
 # ILU(0) 136 (stencil p, z32 -> p, Ap: 28; update x, p, r, Ap -> x, r, r32:
@@ -213,7 +218,10 @@ def run_reference(args):
     # iterations as the FP64 GPU path; the count of the seeded workload at
     # this size is recorded once per run by a short GPU-free estimate: the
     # projection uses the iteration count of the FP64 solve of this workload.
-    ncg = args.ref_iterations or SOLVE_ITERATIONS.get((args.workload, args.ifprec), 6500)
+    ncg = args.ref_iterations or SOLVE_ITERATIONS.get((args.workload, args.ifprec), 0)
+    if ncg <= 0:
+        raise SystemExit(f"no iteration count known for {args.workload} with ifprec {args.ifprec}: "
+                         "give --ref-iterations")
     vals = []
     for _ in range(args.warmup + args.steps):
         cb = cpu_baseline(mesh, br0, opt, args.ifprec, ncg, args.cpu_sample_iters)
