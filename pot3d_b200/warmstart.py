@@ -9,8 +9,8 @@ Training pairs are (Br0 map, phi) of seeded synthetic PFSS cases solved by
 the FP64 GPU PCG (`--train-eps`, default 1e-7: the network is far less
 accurate than that).  The evaluation solves every held-out case to the
 unchanged tolerance (epscg 1e-9) from x = 0 and from the network's guess;
-PCG is the judge either way, so a poor guess costs iterations, never
-accuracy.
+PCG decides convergence either way, so a poor guess costs iterations,
+never accuracy.
 """
 from __future__ import annotations
 
