@@ -1,25 +1,37 @@
 """Benchmark: seconds to solve POT3D's PCG to epsn <= 1e-9 on one B200.
 
-One step = one complete PCG solve of the PFSS workload 255x361x721 (65.3 M
-unknowns, seeded synthetic Br: spherical harmonics l<=40 plus 20 bipoles),
-from a zero guess to the reference's stopping rule epsn < epscg = 1e-9
-(ernorm, src/pot3d.F90:4430-4433).  The default solver is the reference's
-ILU(0) preconditioner (ifprec=2) applied in FP32 by the wavefront sweeps
-inside FP64 PCG; the plain FP64 PCG with the diagonal preconditioner
-(ifprec=1, the reference's default) is timed in the same run and reported
-beside it (`plain_fp64`).
+One step = one complete solve of the PFSS workload 255x361x721 (65.3 M
+unknowns, seeded synthetic Br: spherical harmonics l<=40 plus 20 bipoles)
+to the reference's stopping rule epsn < epscg = 1e-9 (ernorm,
+src/pot3d.F90:4430-4433), by the headline method: the learned initial
+guess (the FNO trained for this grid, its inference inside the timed
+region) followed by FP32-inner / FP64-refined PCG with the reference's
+ILU(0) preconditioner (ifprec=2).  Timed in the same run, on the same
+inputs: the plain FP64 PCG with the diagonal preconditioner (ifprec=1, the
+reference's default) and FP64 PCG with ILU(0) from zero (same
+preconditioner), both to 1e-9.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload NAME] [--ifprec 1|2] [--precision fp64|fp32_refined]
-                    [--no-plain]
+                    [--warm-start auto|off|PATH] [--no-plain] [--no-parity]
 
 value: device time of the solve (CUDA events on the library's stream around
-the PCG initialisation and iterations), inputs resident in HBM.
-e2e: the same solve through the C-ABI with pinned host buffers,
-pot3d_gpu_cgsolve, host<->device copies of x and r included, wall time.
-The working set (~2.6 GB of vectors, plus ~2.5 GB of sweep coefficient
-streams with ILU(0)) is 20x the 126 MB L2, so no flush is needed between
-steps.
+the PCG initialisation and iterations, plus the guess's inference on
+torch's stream), inputs resident in HBM.
+e2e: the same solve through the C-ABI with page-locked host buffers
+(pot3d_gpu_cgsolve), the map upload, the guess download and the
+host<->device copies of x and r inside the timed wall-clock region.
+The working set (about 3 GB of vectors plus 2.5 GB of sweep coefficient
+streams) is 40x the 126 MB L2, so no flush is needed between steps.
+parity: the headline method solved to 1e-11 against FP64 PCG (ILU(0)) to
+1e-11 on the GPU and against the oracle's FP64 solve (tests/golden fixture):
+phi relative L2 and energy relative errors.
+
+The CPU legs (cpu_baseline and --impl reference) time the oracle -- the C
+restatement of the reference's CPU PCG -- on the host cores, on a case the
+oracle builds by itself (its mesh, the seeded map generator and readbr),
+over a bounded sample of PCG iterations projected to the iteration count
+of the oracle's own full solve of the workload (tests/golden fixture).
 
 Multi-GPU: replicas only (each rank solves its own instance); the reported
 time is the maximum over ranks.
@@ -40,22 +52,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "solve s to 1e-9 resid: learned+FP32-refined vs plain FP64 PCG on 1 B200; HBM GB/s"
-# Iteration counts of the seeded workloads' solves from a zero guess (FP64
-# PCG to 1e-9; (workload, ifprec) -> iterations), used to project the
-# reference arm's CPU sample to a whole solve: the GPU solves' counts, and
-# for the two smaller grids the oracle's full solves.
-SOLVE_ITERATIONS = {("pfss_255x361x721", 1): 7036, ("pfss_255x361x721", 2): 1094,
-                    ("pfss_63x91x181", 1): 1302, ("pfss_63x91x181", 2): 273,
-                    ("pfss_127x181x361", 1): 3064,
-                    ("open_511x721x1441", 1): 15639, ("open_511x721x1441", 2): 2165}
-# Algorithmic DRAM bytes per unknown and PCG iteration: diagonal
-# preconditioner 80 (stencil r, p -> p, Ap; update x, p, r, Ap -> x, r);
-# ILU(0) 136 (stencil p, z32 -> p, Ap: 28; update x, p, r, Ap -> x, r, r32:
-# 52; forward sweep r32, 3 coefficients -> y: 20; backward sweep y, 3
-# coefficients + dinv -> z32: 24; r.z: 12).
-BYTES_PER_UNKNOWN_ITER = {1: 80.0, 2: 136.0}
-SWEEP_BYTES_PER_UNKNOWN = {"k_dilu_wave<fwd>": 20.0, "k_dilu_wave<bwd>": 24.0}
+# Algorithmic DRAM bytes per unknown (matrix-free coefficients, each vector
+# touched once per fused pass): FP64 PCG iteration 80 (ifprec=1) / 104
+# (ifprec=2); FP32-inner iteration 40 / 64; each FP64 reliable update 24.
+# The ILU(0) application moves 12 B forward (r32, d, y) and 12 B backward
+# (y, d, z32).
+BYTES_PER_UNKNOWN_ITER = {("fp64", 1): 80.0, ("fp64", 2): 104.0, ("fp32_refined", 1): 40.0,
+                          ("fp32_refined", 2): 64.0}
+BYTES_PER_REFINE = 24.0
+SWEEP_BYTES_PER_UNKNOWN = {"k_dilu_wave<fwd>": 12.0, "k_dilu_wave<bwd>": 12.0}
 FALLBACK_HBM_GBS = 6650.0
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def peak_hbm():
@@ -81,6 +88,20 @@ def measured_traffic(kernel: str, workload: str):
             except ValueError:
                 return None
     return None
+
+
+def oracle_fixture(workload: str, ifprec: int):
+    """The oracle's full solve of the workload (tests/golden), or None."""
+    p = os.path.join(GOLDEN, f"{workload}_oracle_ifprec{ifprec}.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        rec = json.load(fh)
+    z = np.load(p[:-5] + ".npz")
+    rec["phi_slices"] = z["phi_slices"]
+    rec["slice_i"] = z["slice_i"]
+    rec["stride"] = int(z["stride"])
+    return rec
 
 
 class ClockSampler:
@@ -133,38 +154,76 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def build_case(name: str, rank: int = 0):
+def workload_params(name: str, rank: int = 0):
     from pot3d_b200 import host
     w = dict(host.WORKLOADS[name])
     opt = w.pop("option", "ss")
     dnb = w.pop("do_not_balance_flux", False)
-    seed = replica_seed(w.pop("seed"), rank)
-    mesh, br0 = host.pfss_case(w["nr"], w["nt"], w["np"], w["lmax"], w["nbip"], seed, option=opt,
+    w["seed"] = replica_seed(w["seed"], rank)
+    return w, opt, dnb
+
+
+def build_case(name: str, rank: int = 0):
+    from pot3d_b200 import host
+    w, opt, dnb = workload_params(name, rank)
+    mesh, br0 = host.pfss_case(w["nr"], w["nt"], w["np"], w["lmax"], w["nbip"], w["seed"], option=opt,
                                do_not_balance_flux=dnb)
-    return mesh, br0, opt, seed
+    return mesh, br0, opt, w["seed"]
 
 
-def cpu_baseline(mesh, br0, option, ifprec, ncg_target, sample_iters):
-    """The oracle (CPU restatement of the reference's PCG, OpenMP on the
-    host cores) timed on a bounded sample of the same workload: set-up, RHS
-    and `sample_iters` PCG iterations; the solve time is projected to the
-    iteration count the full solve needs."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    mo = O.Mesh(mesh.nr, mesh.nt, mesh.np, *[getattr(mesh, f) for f in O.MESH_FIELDS])
+    return O
+
+
+def oracle_case(name: str, seed: int, option: str, dnb: bool):
+    """(mesh, br0) of the workload built by the oracle alone (no product
+    library involved)."""
+    O = _oracle()
+    from pot3d_b200 import host  # workload table only (pure Python)
+    w = host.WORKLOADS[name]
+    return O.pfss_case(w["nr"], w["nt"], w["np"], w["lmax"], w["nbip"], seed, option=option,
+                       do_not_balance_flux=dnb)
+
+
+def cpu_reference_time(workload, ifprec, sample_iters, rank=0):
+    """The oracle (CPU restatement of the reference's PCG, OpenMP on the
+    host cores; the ILU(0) sweeps sequential as in lusol) on the workload:
+    the full solve when it is small, otherwise `sample_iters` iterations
+    projected to the iteration count of the oracle's full solve."""
+    O = _oracle()
+    w, opt, dnb = workload_params(workload, rank)
     t0 = time.perf_counter()
-    s = O.Solver(mo, br0, option, ifprec)
+    mesh, br0 = oracle_case(workload, w["seed"], opt, dnb)
+    s = O.Solver(mesh, br0, option=opt, ifprec=ifprec)
     b = s.rhs()
     t1 = time.perf_counter()
-    out = s.cgsolve(np.zeros(s.N), b, ncgmax=sample_iters, epscg=0.0)
-    t2 = time.perf_counter()
-    per_it = (t2 - t1) / max(1, out["ncg"])
+    N = s.N
+    fix = oracle_fixture(workload, ifprec) if rank == 0 else None
+    if N <= 2_000_000:  # small grids: the whole solve
+        out = s.cgsolve(np.zeros(N), b, epscg=1e-9)
+        t2 = time.perf_counter()
+        rec = {"value": t2 - t1, "unit": "s", "cores": O.threads(), "kind": "port", "projected": False,
+               "sample": f"oracle full PCG solve (ifprec={ifprec}) of {mesh.nr}x{mesh.nt}x{mesh.np} to 1e-9: "
+                         f"{out['ncg']} iterations (set-up {t1 - t0:.1f} s not included)",
+               "iterations": out["ncg"]}
+    else:
+        if fix is None or fix.get("iterations_to_1e-9") is None:
+            raise SystemExit(f"no oracle solve of {workload} (ifprec {ifprec}) in tests/golden: run "
+                             f"tests/golden/make_c2_oracle.py")
+        ncg_full = int(fix["iterations_to_1e-9"])
+        out = s.cgsolve(np.zeros(N), b, ncgmax=sample_iters, epscg=0.0)
+        t2 = time.perf_counter()
+        per_it = (t2 - t1) / max(1, out["ncg"])
+        rec = {"value": per_it * ncg_full, "unit": "s", "cores": O.threads(), "kind": "port", "projected": True,
+               "sample": f"oracle PCG (ifprec={ifprec}) on {mesh.nr}x{mesh.nt}x{mesh.np}: set-up, then "
+                         f"{out['ncg']} iterations timed ({per_it * 1e3:.0f} ms each), projected to the "
+                         f"{ncg_full} iterations of the oracle's own full solve to 1e-9 (tests/golden); "
+                         f"set-up {t1 - t0:.1f} s not included",
+               "iterations": ncg_full, "seconds_per_iteration": per_it}
     del s
-    return {"value": per_it * ncg_target, "unit": "s", "cores": O.threads(), "kind": "port",
-            "sample": f"oracle PCG set-up + {out['ncg']} iterations on {mesh.nr}x{mesh.nt}x{mesh.np}, "
-                      f"{per_it * 1e3:.1f} ms/iteration, projected to {ncg_target} iterations "
-                      f"(set-up {t1 - t0:.1f} s not included)",
-            "seconds_per_iteration": per_it}
+    return rec
 
 
 def dist_init(backend=None):
@@ -210,31 +269,28 @@ def barrier(ws):
 
 
 def run_reference(args):
-    ws, rank, _ = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
+    """The reference's CPU PCG (the oracle) on the same workload: rank 0
+    only; one bounded sample, projected (see cpu_reference_time)."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    mesh, br0, opt, seed = build_case(args.workload)
-    # The reference's CPU path (oracle restatement) needs about as many
-    # iterations as the FP64 GPU path; the count of the seeded workload at
-    # this size is recorded once per run by a short GPU-free estimate: the
-    # projection uses the iteration count of the FP64 solve of this workload.
-    ncg = args.ref_iterations or SOLVE_ITERATIONS.get((args.workload, args.ifprec), 0)
-    if ncg <= 0:
-        raise SystemExit(f"no iteration count known for {args.workload} with ifprec {args.ifprec}: "
-                         "give --ref-iterations")
-    vals = []
-    for _ in range(args.warmup + args.steps):
-        cb = cpu_baseline(mesh, br0, opt, args.ifprec, ncg, args.cpu_sample_iters)
-        vals.append(cb["value"])
-    v = float(np.mean(vals[args.warmup:]))
+    cb = cpu_reference_time(args.workload, args.ifprec, args.ref_sample_iters)
+    v = cb["value"]
+    w, opt, _ = workload_params(args.workload)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "ifprec": args.ifprec, "epscg": 1e-9, "seed": seed,
-                       "parallelism": "replicas"},
-            "cpu_baseline": cb, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": args.workload, "ifprec": args.ifprec, "epscg": args.epscg, "seed": w["seed"],
+                       "option": opt, "parallelism": "replicas",
+                       "method": "the reference's CPU cgsolve from zero (FP64, ILU(0) sweeps sequential)"},
+            "projected": cb["projected"], "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
 def main():
@@ -245,25 +301,26 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pfss_255x361x721")
     ap.add_argument("--ifprec", type=int, default=2)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"])
+    ap.add_argument("--precision", default="fp32_refined", choices=["fp64", "fp32_refined"])
     ap.add_argument("--epscg", type=float, default=1e-9)
     ap.add_argument("--cpu-sample-iters", type=int, default=0,
-                    help="PCG iterations of the CPU sample (0: 20 with the diagonal preconditioner, 6 with ILU(0), "
-                         "whose sequential sweeps take seconds per iteration)")
-    ap.add_argument("--ref-iterations", type=int, default=0,
-                    help="iteration count used to project the CPU sample (0: take it from a GPU solve)")
+                    help="oracle PCG iterations of the CPU baseline sample (0: 10 with ILU(0), whose sequential "
+                         "sweeps take seconds per iteration, 60 with the diagonal preconditioner)")
+    ap.add_argument("--ref-sample-iters", type=int, default=30,
+                    help="oracle PCG iterations of the reference arm's sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warm-start", default="auto",
                     help="FNO weights (.npz) for the learned initial guess; 'auto' uses "
                          "pot3d_b200/weights/fno_<workload>.npz when present; 'off' solves from zero")
     ap.add_argument("--no-plain", action="store_true",
-                    help="skip the plain FP64 PCG (ifprec=1) solve timed beside the headline solve")
+                    help="skip the FP64 solves timed beside the headline solve")
+    ap.add_argument("--no-parity", action="store_true", help="skip the 1e-11 parity solves")
     ap.add_argument("--kernel-timing-only", action="store_true",
                     help="time the hot kernels briefly (stencil and update, or with --ifprec 2 the two "
                          "ILU(0) sweeps; used for ncu captures) and exit")
     args = ap.parse_args()
     if args.cpu_sample_iters <= 0:
-        args.cpu_sample_iters = 6 if args.ifprec == 2 else 20
+        args.cpu_sample_iters = 10 if args.ifprec == 2 else 60
 
     if args.impl == "reference":
         return run_reference(args)
@@ -321,7 +378,7 @@ def main():
         ev1.synchronize()
         return ev0.elapsed_time(ev1) * 1e-3, LAUNCHES[0] - n0
 
-    def solve_resident(learned=True):
+    def solve_resident(solver=s, learned=True, epscg=args.epscg):
         t_inf, n_inf = 0.0, 0
         if model is not None and learned:
             t_inf, n_inf = guess_into(xt)
@@ -329,26 +386,27 @@ def main():
             xt.zero_()
         rt.copy_(bt)
         torch.cuda.synchronize()
-        ierr = s.cgsolve_dev(xt, rt, epscg=args.epscg)
-        inf = s.last_info
-        return ierr, inf.seconds + t_inf, inf.ncg, inf.epsn, inf.true_resid, inf.kernel_launches + n_inf, inf.n_refine
+        ierr = solver.cgsolve_dev(xt, rt, epscg=epscg)
+        inf = solver.last_info
+        return dict(ierr=ierr, seconds=inf.seconds + t_inf, ncg=inf.ncg, epsn=inf.epsn, true_resid=inf.true_resid,
+                    launches=inf.kernel_launches + n_inf, n_refine=inf.n_refine, inference_s=t_inf)
 
     for _ in range(args.warmup):
         solve_resident()
     barrier(ws)
     torch.cuda.synchronize()
-    dev_times, ncgs, launches = [], [], 0
+    steps = []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            ierr, sec, ncg, epsn, tres, nl, nref = solve_resident()
-            if ierr != 0:
-                raise SystemExit(f"solve did not converge (ierr={ierr})")
-            dev_times.append(sec)
-            ncgs.append(ncg)
-            launches += nl
+            st = solve_resident()
+            if st["ierr"] != 0:
+                raise SystemExit(f"solve did not converge (ierr={st['ierr']})")
+            steps.append(st)
     torch.cuda.synchronize()
     barrier(ws)
-    t_dev = reduce_max(float(np.mean(dev_times)), ws)
+    t_dev = reduce_max(float(np.mean([q["seconds"] for q in steps])), ws)
+    x_timed = xt.cpu().numpy()
+    fallback = s.refine_info()[1] if args.precision == "fp32_refined" else 0
 
     # End to end through the host-pointer C-ABI (H2D + solve + D2H) on pinned
     # host buffers; with the learned guess also the map's upload and the
@@ -368,7 +426,8 @@ def main():
             x_pin.copy_(xt)
         else:
             x_h[:] = 0.0
-        s.cgsolve(x_h, r_h, epscg=args.epscg)
+        if s.cgsolve(x_h, r_h, epscg=args.epscg) != 0:
+            raise SystemExit("e2e solve did not converge")
         e2e.append(time.perf_counter() - t0)
     if model is not None:
         h2d += 4 * br0n_h.numel()
@@ -376,62 +435,96 @@ def main():
         check_errors()
     t_e2e = reduce_max(float(np.mean(e2e)), ws)
 
-    # The same solver from a zero guess (what the learned guess saves).
+    # The same method from a zero guess (what the learned guess saves).
     zero_guess = None
     if model is not None:
-        ierr0, sec0, ncg0, *_ = solve_resident(learned=False)
-        zero_guess = {"seconds": reduce_max(sec0, ws), "iterations": ncg0}
+        z0 = solve_resident(learned=False)
+        zero_guess = {"seconds": reduce_max(z0["seconds"], ws), "iterations": z0["ncg"]}
 
     # Live kernel timing (CUDA events on the library's stream).
     kern = None
-    if args.precision == "fp64" and args.ifprec != 2:
-        ms, by = s.time_kernels(20)
-        kern = {"k_stencil": {"ms": ms[0], "bytes": by[0], "gbs": by[0] / (ms[0] * 1e-3) / 1e9},
-                "k_update": {"ms": ms[1], "bytes": by[1], "gbs": by[1] / (ms[1] * 1e-3) / 1e9}}
-    elif args.ifprec == 2:
+    if args.ifprec == 2:
         fms, bms = s.time_sweeps(10)
         kern = {}
         for name, t in (("k_dilu_wave<fwd>", fms), ("k_dilu_wave<bwd>", bms)):
             by = SWEEP_BYTES_PER_UNKNOWN[name] * N
             kern[name] = {"ms": t, "bytes": by, "gbs": by / (t * 1e-3) / 1e9}
+    elif args.precision == "fp64":
+        ms, by = s.time_kernels(20)
+        kern = {"k_stencil": {"ms": ms[0], "bytes": by[0], "gbs": by[0] / (ms[0] * 1e-3) / 1e9},
+                "k_update": {"ms": ms[1], "bytes": by[1], "gbs": by[1] / (ms[1] * 1e-3) / 1e9}}
 
-    # The plain FP64 PCG (diagonal preconditioner) on the same inputs.
-    plain = None
-    if args.ifprec == 2 and not args.no_plain:
+    # FP64 PCG beside it: ILU(0) from zero (same preconditioner) and the
+    # diagonal preconditioner (the reference's default), same inputs.
+    plain = same_prec = None
+    s64 = None
+    if not args.no_plain or not args.no_parity:
+        s64 = Pot3dSolver(mesh, br0, option=opt, ifprec=2, precision="fp64", device=local)
+    if not args.no_plain:
+        r64 = [solve_resident(s64, learned=False) for _ in range(2 if args.warmup > 0 else 1)]
+        same_prec = {"seconds": reduce_max(r64[-1]["seconds"], ws), "iterations": r64[-1]["ncg"], "ifprec": 2,
+                     "precision": "fp64", "initial_guess": "zero", "speedup": reduce_max(r64[-1]["seconds"], ws) / t_dev}
         sp = Pot3dSolver(mesh, br0, option=opt, ifprec=1, precision="fp64", device=local)
-        pt = []
-        for it in range(2 if args.warmup > 0 else 1):
-            xt.zero_()
-            rt.copy_(bt)
-            torch.cuda.synchronize()
-            if sp.cgsolve_dev(xt, rt, epscg=args.epscg) != 0:
-                raise SystemExit("plain FP64 solve did not converge")
-            pt.append(sp.last_info.seconds)
-        p_ncg = sp.last_info.ncg
+        pt = [solve_resident(sp, learned=False) for _ in range(2 if args.warmup > 0 else 1)]
         sp.close()
-        t_plain = reduce_max(pt[-1], ws)
-        plain = {"seconds": t_plain, "iterations": p_ncg, "ifprec": 1, "precision": "fp64",
-                 "speedup": t_plain / t_dev}
+        if any(q["ierr"] for q in pt + r64):
+            raise SystemExit("an FP64 solve did not converge")
+        t_plain = reduce_max(pt[-1]["seconds"], ws)
+        plain = {"seconds": t_plain, "iterations": pt[-1]["ncg"], "ifprec": 1, "precision": "fp64",
+                 "initial_guess": "zero", "speedup": t_plain / t_dev,
+                 "achieved_gbs": 80.0 * N * pt[-1]["ncg"] / t_plain / 1e9}
+
+    # Parity: the headline method and FP64 PCG both to 1e-11; the timed 1e-9
+    # solution against the FP64 1e-11 one; energies against the oracle's.
+    parity = None
+    if not args.no_parity:
+        def fields(x):
+            out = s.fields(x, want=("phi", "w"))
+            return out["phi"], out["w"]
+        ref = solve_resident(s64, learned=False, epscg=1e-11)
+        x64 = xt.cpu().numpy()
+        mine = solve_resident(s, learned=True, epscg=1e-11)
+        x11 = xt.cpu().numpy()
+        phi64, w64 = fields(x64)
+        phi11, w11 = fields(x11)
+        phi9, w9 = fields(x_timed)
+        parity = {"epscg": 1e-11, "fp64_ilu_iterations": ref["ncg"], "method_iterations": mine["ncg"],
+                  "phi_rel_l2": rel_l2(phi11, phi64), "energy_rel_err": float(np.max(np.abs(w11 - w64) / np.abs(w64))),
+                  "timed_1e-9_phi_rel_l2": rel_l2(phi9, phi64),
+                  "timed_1e-9_energy_rel_err": float(np.max(np.abs(w9 - w64) / np.abs(w64))),
+                  "energies_1e-11": w11.tolist()}
+        fix = oracle_fixture(args.workload, 1) if rank == 0 else None
+        if fix is not None:
+            wo = np.asarray(fix["energy"])
+            sl = np.stack([phi11[i - 1, ::fix["stride"], ::fix["stride"]] for i in fix["slice_i"]])
+            parity["oracle"] = {"source": f"tests/golden/{args.workload}_oracle_ifprec1 (oracle FP64 PCG to 1e-11)",
+                                "energy_rel_err": float(np.max(np.abs(w11 - wo) / np.abs(wo))),
+                                "phi_slices_rel_l2": rel_l2(sl, fix["phi_slices"])}
+    if s64 is not None:
+        s64.close()
 
     if rank != 0:
         s.close()
         return 0
     peak, psrc = peak_hbm()
-    ncg = int(np.median(ncgs))
-    bytes_per_iter = BYTES_PER_UNKNOWN_ITER[2 if args.ifprec == 2 else 1] * N
-    overall_gbs = bytes_per_iter * ncg / t_dev / 1e9
+    ncg = int(np.median([q["ncg"] for q in steps]))
+    nref = int(np.median([q["n_refine"] for q in steps]))
+    algo_bytes = BYTES_PER_UNKNOWN_ITER[(args.precision, 2 if args.ifprec == 2 else 1)] * N * ncg + \
+        BYTES_PER_REFINE * N * nref
+    overall_gbs = algo_bytes / t_dev / 1e9
     roofline = None
     if kern:
         dom = max(kern, key=lambda k: kern[k]["ms"])
         tr = measured_traffic(dom, args.workload)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
-                    "frac": kern[dom]["gbs"] / peak, "traffic": tr, "peak_source": f"{psrc} (MEASURED_PEAKS.json hbm_gbs)"
-                    if psrc == "measured" else psrc,
+                    "frac": kern[dom]["gbs"] / peak, "traffic": tr,
+                    "peak_source": f"{psrc} (MEASURED_PEAKS.json hbm_gbs)" if psrc == "measured" else psrc,
                     "algorithmic_bytes_per_launch": kern[dom]["bytes"], "kernels": kern,
-                    "solve_achieved_gbs": overall_gbs, "solve_frac": overall_gbs / peak}
+                    "solve_algorithmic_bytes": algo_bytes, "solve_achieved_gbs": overall_gbs,
+                    "solve_frac": overall_gbs / peak}
     cb = None
     if not args.no_cpu_baseline and ws == 1:
-        cb = cpu_baseline(mesh, br0, opt, args.ifprec, ncg, args.cpu_sample_iters)
+        cb = cpu_reference_time(args.workload, args.ifprec, args.cpu_sample_iters)
         cb.pop("seconds_per_iteration", None)
     line = {
         "metric": METRIC, "value": t_dev, "unit": "s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -439,11 +532,14 @@ def main():
         "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": args.workload, "unknowns": N, "ifprec": args.ifprec, "precision": args.precision,
                    "initial_guess": "learned (FNO)" if model is not None else "zero",
-                   "epscg": args.epscg, "seed": seed, "iterations": ncg, "parallelism": "replicas",
-                   "l2": f"working set ~{(52 if args.ifprec != 2 else 104) * N / 1e9:.1f} GB >> 126 MB L2, no flush"},
+                   "epscg": args.epscg, "seed": seed, "iterations": ncg, "reliable_updates": nref,
+                   "fp64_fallback_iterations": fallback, "parallelism": "replicas",
+                   "l2": f"working set ~{(40 if args.ifprec != 2 else 84) * N / 1e9:.1f} GB >> 126 MB L2, no flush"},
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roofline, "cpu_baseline": cb, "clocks": clk.summary(),
-        "gpu_launches": launches, "true_residual": tres, "epsn": epsn, "plain_fp64": plain,
+        "gpu_launches": int(np.sum([q["launches"] for q in steps])), "true_residual": steps[-1]["true_resid"],
+        "epsn": steps[-1]["epsn"], "inference_s": steps[-1]["inference_s"],
+        "plain_fp64": plain, "fp64_same_preconditioner": same_prec, "parity": parity,
         "warm_start": None if model is None else {"weights": os.path.relpath(wpath, ROOT), "zero_guess": zero_guess},
         "throughput_solves_per_s": ws / t_dev,
     }

@@ -79,8 +79,9 @@ enum { POT3D_PREC_NONE = 0, POT3D_PREC_DIAG = 1, POT3D_PREC_ILU0 = 2 };
 /* Arithmetic of the solve. */
 enum {
   POT3D_FP64 = 0,          /* the reference's classical FP64 PCG */
-  POT3D_FP32_REFINED = 1   /* FP32 stencil/preconditioner inner iterations
-                              inside an FP64 iterative-refinement loop */
+  POT3D_FP32_REFINED = 1   /* FP32-stored inner iterations (p, q, r, the
+                              ILU(0) sweeps; products formed in FP64)
+                              inside FP64 reliable updates of r = b - A x */
 };
 
 typedef struct {
@@ -138,6 +139,21 @@ int pot3d_gpu_cgsolve(pot3d_gpu_solver *s, double *x, double *r, long N, int ncg
 /* Same with DEVICE pointers (the Fortran host's use_device_addr arrays). */
 int pot3d_gpu_cgsolve_dev(pot3d_gpu_solver *s, double *x, double *r, long N, int ncgmax,
                           double epscg, int *ierr, pot3d_solve_info_t *info);
+
+/* Controls of the FP32-inner / FP64-refined solve (precision
+ * POT3D_FP32_REFINED).  A reliable update (r = b - A x in FP64, its
+ * preconditioned norm replacing the FP32 recurrence's) is made once the
+ * recurrence's r.M^-1 r has fallen by refine_ratio (default 1e-4) since the
+ * last one, and whenever the recurrence reports convergence or ncgmax.  An
+ * update whose FP64 r.M^-1 r fell by less than the factor stall_drop
+ * (default 0.5) is stagnant; stall_limit (default 2) stagnant updates in a
+ * row finish the solve with FP64 PCG (same preconditioner) from the current
+ * x.  No counterpart in the reference, whose cgsolve is FP64 throughout
+ * (src/pot3d.F90:4231-4369). */
+int pot3d_gpu_set_refine(pot3d_gpu_solver *s, double refine_ratio, double stall_drop, int stall_limit);
+/* Reliable updates of the last refined solve and the FP64 PCG iterations
+ * after a switch to FP64 (0: the solve finished in the refined mode). */
+int pot3d_gpu_refine_info(const pot3d_gpu_solver *s, int *n_refine, int *fallback_iterations);
 
 /* Residual history of the last solve: epsn after iterations 0..n-1
  * (ernorm's value, src/pot3d.F90:4432-4433).  Returns how many were

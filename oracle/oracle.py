@@ -40,6 +40,7 @@ def lib():
         L.orc_set_mesh.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, dp, dp, C.c_int, dp, dp, C.c_int,
                                    dp, dp, C.c_int, C.c_double]
         L.orc_readbr.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, dp, dp, C.c_int, C.c_int, dp]
+        L.orc_synthetic_br.argtypes = [C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp, dp]
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_int, ip]
         L.orc_destroy.argtypes = [C.c_void_p]
@@ -151,6 +152,32 @@ def readbr(mesh: Mesh, tn, pn, fi, option="ss", do_not_balance_flux=False) -> np
     if rc:
         raise ValueError(f"readbr failed (code {rc})")
     return br0
+
+
+def synthetic_br(seed: int, lmax: int, nbip: int, ntn: int, npn: int):
+    """Seeded synthetic Br map (tn, pn, fi[ntn, npn]); the product's
+    generator restated, so a case can be built with the oracle alone."""
+    tn, pn = np.zeros(ntn), np.zeros(npn)
+    fi = np.zeros((ntn, npn), order="F")
+    rc = lib().orc_synthetic_br(seed, lmax, nbip, ntn, npn, _p(tn), _p(pn), _p(fi))
+    if rc:
+        raise ValueError(f"synthetic_br failed (code {rc})")
+    return tn, pn, fi
+
+
+# Seeded workloads: grid and generator settings (the PFSS law r in [1, 2.5]).
+WORKLOADS = {
+    "pfss_63x91x181": dict(nr=63, nt=91, np=181, lmax=15, nbip=4, seed=1),
+    "pfss_255x361x721": dict(nr=255, nt=361, np=721, lmax=40, nbip=20, seed=2),
+    "pfss_127x181x361": dict(nr=127, nt=181, np=361, lmax=40, nbip=20, seed=1000),
+}
+
+
+def pfss_case(nr, nt, np_, lmax, nbip, seed, option="ss", do_not_balance_flux=False, r1=2.5):
+    """(mesh, br0) of a seeded case built by the oracle alone."""
+    mesh = make_mesh(nr, nt, np_, r1=r1)
+    tn, pn, fi = synthetic_br(seed, lmax, nbip, nt, np_)
+    return mesh, readbr(mesh, tn, pn, fi, option=option, do_not_balance_flux=do_not_balance_flux)
 
 
 class Solver:

@@ -400,6 +400,136 @@ int orc_readbr(const orc_mesh *m, int ntn, int npn, const double *tn, const doub
 }
 
 /* ------------------------------------------------------------------ */
+/* Seeded synthetic Br maps.  Not a reference routine: the reference    */
+/* reads its Br maps from HDF5 files.  This restates the product's      */
+/* generator (pot3d_host_synthetic_br, pot3d_b200/csrc/host_mesh.cpp)   */
+/* operation for operation, so inputs can be built with the oracle      */
+/* alone; tests/test_oracle.py checks the two bit for bit.              */
+/* Spherical harmonics l = 1..lmax (orthonormal, N(0,1)/l^2, scaled to  */
+/* 5 G RMS), nbip Gaussian bipoles (sigma 3 deg, +-50 G), area-weighted */
+/* mean removed; seed -> splitmix64 -> Box-Muller.                      */
+/* ------------------------------------------------------------------ */
+static uint64_t orc_sm_next(uint64_t *s) {
+  uint64_t z = (*s += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+static double orc_sm_uniform(uint64_t *s) { return (double)(orc_sm_next(s) >> 11) * (1.0 / 9007199254740992.0); }
+static double orc_sm_normal(uint64_t *s) {
+  const double u1 = 1.0 - orc_sm_uniform(s);
+  const double u2 = orc_sm_uniform(s);
+  return sqrt(-2.0 * log(u1)) * cos(2.0 * ORC_PI * u2);
+}
+
+int orc_synthetic_br(unsigned long long seed, int lmax, int nbip, int ntn, int npn, double *tn, double *pn,
+                     double *fi) {
+  if (ntn < 3 || npn < 3 || lmax < 1) return 1;
+  uint64_t rng = seed;
+  const int L = lmax, W = lmax + 1;
+  for (int j = 0; j < ntn; j++) tn[j] = ORC_PI * j / (ntn - 1);
+  for (int k = 0; k < npn; k++) pn[k] = 2.0 * ORC_PI * k / (npn - 1);
+  double *ac = calloc((size_t)W * W, sizeof(double)), *as = calloc((size_t)W * W, sizeof(double));
+  double *Fc = malloc(sizeof(double) * (size_t)ntn * W), *Fs = malloc(sizeof(double) * (size_t)ntn * W);
+  double *cm = malloc(sizeof(double) * W), *sm = malloc(sizeof(double) * W);
+  if (!ac || !as || !Fc || !Fs || !cm || !sm) {
+    free(ac); free(as); free(Fc); free(Fs); free(cm); free(sm);
+    return 2;
+  }
+  for (int l = 1; l <= L; l++)
+    for (int m = 0; m <= l; m++) {
+      const double s = 1.0 / ((double)l * l);
+      ac[l * W + m] = orc_sm_normal(&rng) * s;
+      if (m > 0) as[l * W + m] = orc_sm_normal(&rng) * s;
+    }
+  for (int j = 0; j < ntn; j++) {
+    const double x = cos(tn[j]), sx = sin(tn[j]);
+    double p_mm = 1.0 / sqrt(4.0 * ORC_PI);
+    for (int m = 0; m <= L; m++) {
+      if (m > 0) p_mm *= sqrt((2.0 * m + 1.0) / (2.0 * m)) * sx;
+      double pl2 = 0.0, pl1 = p_mm, fc = 0.0, fs = 0.0;
+      const double norm = (m == 0) ? 1.0 : sqrt(2.0);
+      for (int l = m; l <= L; l++) {
+        double pl;
+        if (l == m) {
+          pl = p_mm;
+        } else if (l == m + 1) {
+          pl = sqrt(2.0 * m + 3.0) * x * p_mm;
+        } else {
+          const double a = sqrt((4.0 * l * l - 1.0) / ((double)l * l - (double)m * m));
+          const double b = sqrt(((l - 1.0) * (l - 1.0) - (double)m * m) / (4.0 * (l - 1.0) * (l - 1.0) - 1.0));
+          pl = a * (x * pl1 - b * pl2);
+        }
+        if (l > m) {
+          pl2 = pl1;
+          pl1 = pl;
+        }
+        if (l >= 1) {
+          fc += norm * ac[l * W + m] * pl;
+          fs += norm * as[l * W + m] * pl;
+        }
+        if (l == m) {
+          pl2 = 0.0;
+          pl1 = pl;
+        }
+      }
+      Fc[(size_t)j * W + m] = fc;
+      Fs[(size_t)j * W + m] = fs;
+    }
+  }
+  double wsum = 0.0, ssq = 0.0;
+  for (int k = 0; k < npn; k++) {
+    for (int m = 0; m <= L; m++) {
+      cm[m] = cos(m * pn[k]);
+      sm[m] = sin(m * pn[k]);
+    }
+    for (int j = 0; j < ntn; j++) {
+      double v = 0.0;
+      for (int m = 0; m <= L; m++) v += Fc[(size_t)j * W + m] * cm[m] + Fs[(size_t)j * W + m] * sm[m];
+      fi[j + (size_t)ntn * k] = v;
+      const double w = sin(tn[j]);
+      wsum += w;
+      ssq += w * v * v;
+    }
+  }
+  const double rms = sqrt(ssq / wsum);
+  const double scale = rms > 0 ? 5.0 / rms : 0.0;
+  for (size_t q = 0; q < (size_t)ntn * npn; q++) fi[q] *= scale;
+  const double deg = ORC_PI / 180.0, sig = 3.0 * deg, half_sep = 3.0 * deg;
+  for (int b = 0; b < nbip; b++) {
+    const double lat = (-35.0 + 70.0 * orc_sm_uniform(&rng)) * deg;
+    const double lon = 360.0 * orc_sm_uniform(&rng) * deg;
+    const double tilt = (-20.0 + 40.0 * orc_sm_uniform(&rng)) * deg;
+    const double sgn = orc_sm_uniform(&rng) < 0.5 ? 1.0 : -1.0;
+    for (int side = 0; side < 2; side++) {
+      const double sd = side == 0 ? 1.0 : -1.0;
+      const double slat = lat + sd * half_sep * sin(tilt);
+      const double slon = lon + sd * half_sep * cos(tilt) / cos(lat);
+      const double amp = 50.0 * sgn * sd;
+      const double cl = cos(slat), sl = sin(slat);
+      for (int k = 0; k < npn; k++)
+        for (int j = 0; j < ntn; j++) {
+          const double plat = 0.5 * ORC_PI - tn[j];
+          double c = sl * sin(plat) + cl * cos(plat) * cos(pn[k] - slon);
+          c = c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
+          const double d = acos(c);
+          fi[j + (size_t)ntn * k] += amp * exp(-0.5 * (d * d) / (sig * sig));
+        }
+    }
+  }
+  double num = 0.0;
+  for (int k = 0; k < npn - 1; k++)
+    for (int j = 0; j < ntn; j++) num += sin(tn[j]) * fi[j + (size_t)ntn * k];
+  double den = 0.0;
+  for (int k = 0; k < npn - 1; k++)
+    for (int j = 0; j < ntn; j++) den += sin(tn[j]);
+  const double mean = num / den;
+  for (size_t q = 0; q < (size_t)ntn * npn; q++) fi[q] -= mean;
+  free(ac); free(as); free(Fc); free(Fs); free(cm); free(sm);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* The solve context: coefficients, preconditioner, work arrays.        */
 /* ------------------------------------------------------------------ */
 

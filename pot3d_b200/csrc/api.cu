@@ -292,3 +292,26 @@ extern "C" int pot3d_gpu_set_br0(pot3d_gpu_solver *h, const double *br0) {
   CKS(cudaStreamSynchronize(s.stream));
   return POT3D_OK;
 }
+
+extern "C" int pot3d_gpu_set_refine(pot3d_gpu_solver *h, double refine_ratio, double stall_drop, int stall_limit) {
+  int st;
+  if ((st = check_solver(h))) return st;
+  if (!(refine_ratio > 0.0 && refine_ratio < 1.0) || !(stall_drop > 0.0) || stall_limit < 1) {
+    pot3d_set_error("pot3d_gpu_set_refine: need 0 < refine_ratio < 1, stall_drop > 0, stall_limit >= 1");
+    return POT3D_ERR_ARG;
+  }
+  h->s.refine_ratio = refine_ratio;
+  h->s.stall_drop = stall_drop;
+  h->s.stall_limit = stall_limit;
+  return POT3D_OK;
+}
+
+extern "C" int pot3d_gpu_refine_info(const pot3d_gpu_solver *h, int *n_refine, int *fallback_iterations) {
+  if (!h) {
+    pot3d_set_error("null solver handle");
+    return POT3D_ERR_ARG;
+  }
+  if (n_refine) *n_refine = h->s.last_refine;
+  if (fallback_iterations) *fallback_iterations = h->s.last_fallback_iters;
+  return POT3D_OK;
+}

@@ -141,7 +141,13 @@ __device__ __forceinline__ double apply_fac(const PtFac &f, double dpim, double 
 // Stencil kernel.  MODE_AX: y = A x (ax, src/pot3d.F90:5102-5150) with the
 // south-pole ring sums S1 supplied.  MODE_PCG: p_new = beta*p + a_i*r on the
 // fly, q = A p_new, p_new.q.  MODE_PCGZ: same with z read from an FP32
-// vector (the ILU(0) preconditioner's output).
+// vector (the ILU(0) preconditioner's output).  MODE_PCG32 / MODE_PCGZ32:
+// the FP32-inner forms of PCG / PCGZ: p, r, z and q are stored in FP32 and
+// read as FP32 boxes, but p_new is formed and rounded once, and A p_new is
+// evaluated, in FP64 registers, so q is the FP64 product of the stored
+// FP32 p_new rounded once.  (An FP32 evaluation of a4*x - sum(a_nb*x_nb)
+// cancels away the smooth modes that set the convergence of this
+// operator; FP64 arithmetic costs nothing here, the kernel is HBM-bound.)
 //
 // Boundaries (set_boundary_points with vmask=0, src/pot3d.F90:5413-5484):
 //   i=1  ghost = x(2)            (r0 Neumann)
@@ -150,7 +156,7 @@ __device__ __forceinline__ double apply_fac(const PtFac &f, double dpim, double 
 //   j=nt ghost = 2*S1(i) - x(i,ntm1,k), S1 the ring mean of x at j=ntm1
 //   k    periodic wrap (seam_hhh, src/pot3d.F90:5746-5758)
 // ============================================================================
-enum { MODE_AX = 0, MODE_PCG = 1, MODE_PCGZ = 2, MODE_PCG32 = 3 };
+enum { MODE_AX = 0, MODE_PCG = 1, MODE_PCGZ = 2, MODE_PCG32 = 3, MODE_PCGZ32 = 4 };
 
 struct StencilArgs {
   const double *x;          // AX input
@@ -208,6 +214,10 @@ template <>
 struct StageCfg<MODE_PCG32> {
   static constexpr int n64 = 0, n32 = 3;
 };
+template <>
+struct StageCfg<MODE_PCGZ32> {
+  static constexpr int n64 = 0, n32 = 2;
+};
 template <int MODE>
 struct StageLayout {
   static constexpr int n64 = StageCfg<MODE>::n64, n32 = StageCfg<MODE>::n32;
@@ -217,7 +227,8 @@ struct StageLayout {
   static constexpr int smem = kfac_off + 3 * 8 * MAX_TK;
 };
 
-// Tensor maps of the stage inputs: m64[0] = x | p_old, m64[1] = r, m32 = a_i | z.
+// Tensor maps of the stage inputs: m64[0] = x | p_old, m64[1] = r, m32 = a_i | z;
+// FP32 modes: m32[0] = p_old, m32[1] = r (PCG32) | z (PCGZ32), m32[2] = a_i (PCG32).
 struct StencilMaps {
   CUtensorMap m64[2];
   CUtensorMap m32[3];
@@ -234,28 +245,17 @@ struct Vec2<float> {
   using type = float2;
 };
 
-template <typename T>
-__device__ __forceinline__ T apply_fac_t(const PtFac &f, T dpim, T dpip, T dphk, T xkm, T xjm, T xim, T xc, T xip,
-                                         T xjp, T xkp) {
-  if constexpr (sizeof(T) == 8) {
-    return apply_fac(f, dpim, dpip, dphk, xkm, xjm, xim, xc, xip, xjp, xkp);
-  } else {
-    const float g1 = (float)f.g1, g2 = (float)f.g2, g3 = (float)f.g3, g5 = (float)f.g5, g6 = (float)f.g6,
-                gs = (float)f.gs;
-    const float a4 = fmaf(g1, dpim + dpip, gs * dphk);
-    const float tk = fmaf(dpim, xkm, dpip * xkp);
-    const float tr = fmaf(g3, xim, g5 * xip);
-    const float tt = fmaf(g2, xjm, g6 * xjp);
-    const float off = fmaf(g1, tk, dphk * (tr + tt));
-    return fmaf(a4, xc, -off);
-  }
+template <typename T2>
+__device__ __forceinline__ double2 widen2(const T2 v) {
+  return make_double2((double)v.x, (double)v.y);
 }
 
 template <int MODE>
 __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo &g, const DevMesh &m,
                                              const StencilArgs &a, const int bx, const int by, const int bz) {
   using L = StageLayout<MODE>;
-  using T = typename std::conditional<MODE == MODE_PCG32, float, double>::type;
+  constexpr bool F32 = MODE == MODE_PCG32 || MODE == MODE_PCGZ32;
+  using T = typename std::conditional<F32, float, double>::type;  // storage of p_new and q
   using T2 = typename Vec2<T>::type;
   extern __shared__ __align__(1024) unsigned char dyn[];
   __shared__ __align__(8) uint64_t bar[S_STAGES];
@@ -350,8 +350,8 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
   const double pm = m.pm_r1;
   double dot = 0.0;
 
-  // p_new at (row, col) of the stage tile; col counts FP64 columns.
-  const float betaf = (float)beta;
+  // p_new at (row, col) of the stage tile; col counts FP64 columns.  The
+  // FP32 modes form it in FP64 and round it once.
   auto pnew_at = [&](const unsigned char *st, int row, int col) -> T {
     const double *t0 = reinterpret_cast<const double *>(st);
     if constexpr (MODE == MODE_PCG32) {
@@ -359,7 +359,12 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
       const float *f1 = reinterpret_cast<const float *>(st + TILE32_PITCH);
       const float *f2 = reinterpret_cast<const float *>(st + 2 * TILE32_PITCH);
       const int c = row * BOX32_X + col + 2;
-      return fmaf(betaf, f0[c], f2[c] * f1[c]);
+      return (float)fma(beta, (double)f0[c], (double)f2[c] * (double)f1[c]);
+    } else if constexpr (MODE == MODE_PCGZ32) {
+      const float *f0 = reinterpret_cast<const float *>(st);
+      const float *f1 = reinterpret_cast<const float *>(st + TILE32_PITCH);
+      const int c = row * BOX32_X + col + 2;
+      return (float)fma(beta, (double)f0[c], (double)f1[c]);
     } else if (MODE == MODE_AX) {
       return t0[row * BOX64_X + col];
     } else if (MODE == MODE_PCG) {
@@ -409,42 +414,41 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
       const T *sm = pn_ring + ((local - 2) % PN_SLOTS) * (BOX_Y * BOX64_X);
       const T *sp = slot;
       const int kq = kk - k0;
-      const T dpim = (T)kfac[3 * kq], dpip = (T)kfac[3 * kq + 1], dphk = (T)kfac[3 * kq + 2];
+      const double dpim = kfac[3 * kq], dpip = kfac[3 * kq + 1], dphk = kfac[3 * kq + 2];
       const int col = 2 + el;
       const T *rowc = sc + (w + 1) * BOX64_X;
-      const T2 xc = *reinterpret_cast<const T2 *>(rowc + col);
-      const T2 xm = *reinterpret_cast<const T2 *>(sm + (w + 1) * BOX64_X + col);
-      const T2 xn = *reinterpret_cast<const T2 *>(sp + (w + 1) * BOX64_X + col);
-      const T2 xjm2 = *reinterpret_cast<const T2 *>(sc + w * BOX64_X + col);
-      const T2 xjp2 = *reinterpret_cast<const T2 *>(sc + (w + 2) * BOX64_X + col);
-      const T pmT = (T)pm, two = (T)2;
-      const T xim = (e0 == 0) ? xc.x : rowc[col - 1];
-      const T xip = (e0 == g.nrm2 - 1) ? pmT * xc.x : xc.y;
-      const T xjm = (jj == 0) ? (T)0 : xjm2.x;
-      const T xjp = south ? two * (T)s1a - xc.x : xjp2.x;
-      const T y = apply_fac_t<T>(f0, dpim, dpip, dphk, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
-      T y1 = (T)0;
+      const T2 xcT = *reinterpret_cast<const T2 *>(rowc + col);
+      const double2 xc = widen2(xcT);
+      const double2 xm = widen2(*reinterpret_cast<const T2 *>(sm + (w + 1) * BOX64_X + col));
+      const double2 xn = widen2(*reinterpret_cast<const T2 *>(sp + (w + 1) * BOX64_X + col));
+      const double2 xjm2 = widen2(*reinterpret_cast<const T2 *>(sc + w * BOX64_X + col));
+      const double2 xjp2 = widen2(*reinterpret_cast<const T2 *>(sc + (w + 2) * BOX64_X + col));
+      const double xim = (e0 == 0) ? xc.x : (double)rowc[col - 1];
+      const double xip = (e0 == g.nrm2 - 1) ? pm * xc.x : xc.y;
+      const double xjm = (jj == 0) ? 0.0 : xjm2.x;
+      const double xjp = south ? 2.0 * s1a - xc.x : xjp2.x;
+      const double y = apply_fac(f0, dpim, dpip, dphk, xm.x, xjm, xim, xc.x, xip, xjp, xn.x);
+      double y1 = 0.0;
       if (v1) {
-        const T xip1 = (e0 + 1 == g.nrm2 - 1) ? pmT * xc.y : rowc[col + 2];
-        const T xjm1 = (jj == 0) ? (T)0 : xjm2.y;
-        const T xjp1 = south ? two * (T)s1b - xc.y : xjp2.y;
-        y1 = apply_fac_t<T>(f1, dpim, dpip, dphk, xm.y, xjm1, xc.x, xc.y, xip1, xjp1, xn.y);
+        const double xip1 = (e0 + 1 == g.nrm2 - 1) ? pm * xc.y : (double)rowc[col + 2];
+        const double xjm1 = (jj == 0) ? 0.0 : xjm2.y;
+        const double xjp1 = south ? 2.0 * s1b - xc.y : xjp2.y;
+        y1 = apply_fac(f1, dpim, dpip, dphk, xm.y, xjm1, xc.x, xc.y, xip1, xjp1, xn.y);
       }
       const long long id = g.idx(e0, jj, kk);
-      T2 yv;
-      yv.x = y;
-      yv.y = y1;
-      T2 own;
-      own.x = xc.x;
-      own.y = v1 ? xc.y : (T)0;
       if constexpr (MODE == MODE_AX) {
-        *reinterpret_cast<double2 *>(a.y + id) = yv;
-      } else if constexpr (MODE == MODE_PCG32) {
-        *reinterpret_cast<float2 *>(a.q32 + id) = yv;
+        *reinterpret_cast<double2 *>(a.y + id) = make_double2(y, y1);
+      } else if constexpr (F32) {
+        // q is stored rounded; p.q uses the stored values, as the update does
+        const float2 qv = make_float2((float)y, (float)y1);
+        const float2 own = make_float2(xcT.x, v1 ? xcT.y : 0.0f);
+        *reinterpret_cast<float2 *>(a.q32 + id) = qv;
         *reinterpret_cast<float2 *>(a.p_new32 + id) = own;
-        dot = fma((double)own.x, (double)y, dot);
-        dot = fma((double)own.y, (double)y1, dot);
+        dot = fma((double)own.x, (double)qv.x, dot);
+        dot = fma((double)own.y, (double)qv.y, dot);
       } else {
+        double2 yv = make_double2(y, y1);
+        double2 own = make_double2(xc.x, v1 ? xc.y : 0.0);
         *reinterpret_cast<double2 *>(a.q + id) = yv;
         *reinterpret_cast<double2 *>(a.p_new + id) = own;
         dot = fma(own.x, y, dot);
@@ -482,11 +486,12 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
   }
 }
 
-// The PCGZ stages (one FP64 and one FP32 box per plane) fit three blocks per
-// SM in shared memory, so that mode is compiled for three; the others hold
-// more per stage and stay at two (a tighter register cap only slows them).
+// The PCGZ stages (one FP64 and one FP32 box per plane) and the PCGZ32
+// stages (two FP32 boxes) fit three blocks per SM in shared memory, so those
+// modes are compiled for three; the others hold more per stage and stay at
+// two (a tighter register cap only slows them).
 template <int MODE>
-__global__ void __launch_bounds__(NTHR, MODE == MODE_PCGZ ? 3 : 2)
+__global__ void __launch_bounds__(NTHR, (MODE == MODE_PCGZ || MODE == MODE_PCGZ32) ? 3 : 2)
     k_stencil(const __grid_constant__ StencilMaps maps, Geo g, DevMesh m, StencilArgs a) {
   stencil_body<MODE>(maps, g, m, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
@@ -505,15 +510,22 @@ struct UpdateArgs {
   const double *q;
   const float *ai;
   const float *z32;       // ILU(0) output (ifprec=2); ai is then unused
-  float *r32;             // ifprec=2: FP32 copy of r for the sweeps
+  float *r32;             // ifprec=2: FP32 copy of r for the sweeps; R32: the residual itself
+  const float *p32;       // R32: FP32 search direction and A p
+  const float *q32;
   double *s1z_part;       // [nkc][NRP]
   SolveState *st;
   double *partials;
 };
 // UPD_ZDOT: r.z with z from the ILU(0) sweeps, ncg+1 and ernorm, no update.
-enum { UPD_ITER = 0, UPD_INIT = 1, UPD_BDOTB = 2, UPD_ZDOT = 3 };
+// UPD_RU: r.z of a freshly computed FP64 residual (a reliable update of the
+// FP32-inner solve): rho and beta are replaced, ncg does not advance, and
+// the status is decided on this residual whatever the recurrence said.
+enum { UPD_ITER = 0, UPD_INIT = 1, UPD_BDOTB = 2, UPD_ZDOT = 3, UPD_RU = 4 };
 
-template <int KIND, bool ZIN>
+// R32: the residual (and, for UPD_ITER, p and q) are FP32 vectors; the
+// arithmetic is FP64 and the new residual is rounded once when stored.
+template <int KIND, bool ZIN, bool R32 = false>
 __device__ __forceinline__ void update_body(const Geo &g, const DevMesh &m, const UpdateArgs &a, const int bx,
                                             const int by, const int bz) {
   __shared__ double red[NTHR / 32];
@@ -533,17 +545,26 @@ __device__ __forceinline__ void update_body(const Geo &g, const DevMesh &m, cons
 #pragma unroll 4
     for (int kk = k0; kk < k1; kk++) {
       const long long id = g.idx(e0, jj, kk);
-      double2 rv = *reinterpret_cast<const double2 *>(a.r + id);
+      double2 rv = R32 ? widen2(*reinterpret_cast<const float2 *>(a.r32 + id))
+                       : *reinterpret_cast<const double2 *>(a.r + id);
       if (KIND == UPD_ITER) {
         double2 xv = *reinterpret_cast<const double2 *>(a.x + id);
-        const double2 pv = __ldg(reinterpret_cast<const double2 *>(a.p + id));
-        const double2 qv = __ldg(reinterpret_cast<const double2 *>(a.q + id));
+        const double2 pv = R32 ? widen2(__ldg(reinterpret_cast<const float2 *>(a.p32 + id)))
+                               : __ldg(reinterpret_cast<const double2 *>(a.p + id));
+        const double2 qv = R32 ? widen2(__ldg(reinterpret_cast<const float2 *>(a.q32 + id)))
+                               : __ldg(reinterpret_cast<const double2 *>(a.q + id));
         xv.x = fma(alpha, pv.x, xv.x);
         xv.y = fma(alpha, pv.y, xv.y);
         rv.x = fma(-alpha, qv.x, rv.x);
         rv.y = fma(-alpha, qv.y, rv.y);
         *reinterpret_cast<double2 *>(a.x + id) = xv;
-        *reinterpret_cast<double2 *>(a.r + id) = rv;
+        if (R32) {
+          const float2 r2 = make_float2((float)rv.x, (float)rv.y);
+          *reinterpret_cast<float2 *>(a.r32 + id) = r2;
+          rv = widen2(r2);  // r.z of the stored residual
+        } else {
+          *reinterpret_cast<double2 *>(a.r + id) = rv;
+        }
       }
       if (!v1) rv.y = 0.0;
       double zx, zy;
@@ -580,7 +601,8 @@ __device__ __forceinline__ void update_body(const Geo &g, const DevMesh &m, cons
       if (KIND == UPD_BDOTB) {
         s->bdotb = total;
       } else {
-        s->rho_old = s->rho;
+        const double rho_it = s->rho;  // UPD_RU: the recurrence's value it replaces
+        if (KIND != UPD_RU) s->rho_old = s->rho;
         s->rho = total;
         if (KIND == UPD_ITER || KIND == UPD_ZDOT) s->ncg = s->ncg + 1;
         // ernorm
@@ -588,6 +610,7 @@ __device__ __forceinline__ void update_body(const Geo &g, const DevMesh &m, cons
         const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
         s->epsn = epsn;
         if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
+        if (KIND == UPD_RU) s->status = ST_RUNNING;
         if (epsn < s->epscg) {
           s->status = ST_CONVERGED;
         } else if (s->ncg >= s->ncgmax) {
@@ -595,15 +618,19 @@ __device__ __forceinline__ void update_body(const Geo &g, const DevMesh &m, cons
         } else if (!isfinite(epsn)) {
           s->status = ST_BREAKDOWN;
         }
-        s->beta = (KIND == UPD_INIT) ? 0.0 : total / s->rho_old;
+        if (KIND == UPD_RU) s->rho_true = total;
+        // a reliable update that finds the recurrence far off (its r.z more
+        // than 10x the recurrence's) restarts the direction: p = z
+        const bool restart = KIND == UPD_RU && (!(s->rho_old > 0.0) || total > 10.0 * rho_it);
+        s->beta = (KIND == UPD_INIT || restart) ? 0.0 : total / s->rho_old;
       }
     }
   }
 }
 
-template <int KIND, bool ZIN>
+template <int KIND, bool ZIN, bool R32 = false>
 __global__ void __launch_bounds__(NTHR) k_update(Geo g, DevMesh m, UpdateArgs a) {
-  update_body<KIND, ZIN>(g, m, a, blockIdx.x, blockIdx.y, blockIdx.z);
+  update_body<KIND, ZIN, R32>(g, m, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ifprec=2 half of the update: x += alpha p ; r -= alpha q ; r32 = (float)r
@@ -638,136 +665,56 @@ __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__r
 }
 
 // ============================================================================
-// FP32-inner / FP64-refined PCG.  Inner iterations keep p, r, q and the
-// solution correction xs in FP32 and do the stencil and the preconditioner
-// in FP32; every dot product is accumulated in FP64 and alpha, beta stay
-// FP64 on the device.  A reliable update folds xs into the FP64 solution,
-// recomputes the true residual b - A x in FP64 and its preconditioned norm
-// (the reference's epsn), and restarts the recurrence residual from it while
-// keeping the search direction.  Convergence is decided on that true epsn.
+// FP32-inner / FP64-refined PCG (both preconditioners).  The inner
+// iterations keep p, q and the recurrence residual r in FP32 (half the bytes
+// of the FP64 iteration) while every product is formed in FP64 registers:
+// the stencil (MODE_PCG32 / MODE_PCGZ32), alpha, beta and the dots
+// (accumulated in FP64), and the solution update x += alpha p on the FP64 x.
+// A reliable update recomputes r = b - A x in FP64 and its preconditioned
+// norm (the reference's epsn, src/pot3d.F90:4432-4433), replaces the
+// recurrence's rho with it and keeps the search direction; convergence is
+// only ever accepted on that FP64 residual.
 // ============================================================================
-struct Update32Args {
-  float *xs;
-  const float *p;
-  float *r;
-  const float *q;
-  const float *ai;
-  double *s1z_part;
-  SolveState *st;
-  double *partials;
-};
-enum { U32_ITER = 0, U32_RESTART = 1 };
 
-template <int KIND>
-__global__ void __launch_bounds__(NTHR) k_update32(Geo g, DevMesh m, Update32Args a) {
-  __shared__ double red[NTHR / 32];
+// ILU(0) inner update: x += alpha p (FP64 x, FP32 p), r32 = r32 - alpha q
+// rounded once; the sweeps then read r32 directly.  Four unknowns per thread
+// (the padded vector length is a multiple of 16).
+__global__ void __launch_bounds__(NTHR) k_update_x32(Geo g, UpdateArgs a) {
   const volatile SolveState *vs = a.st;
-  if (KIND == U32_ITER && vs->status != ST_RUNNING) return;
-  const float alpha = (KIND == U32_ITER) ? (float)vs->alpha : 0.0f;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int e0 = blockIdx.x * TI + 2 * lane;
-  const int jj = blockIdx.y * TJ + w;
-  const int k0 = blockIdx.z * g.tk_u;
-  const int k1 = min(k0 + g.tk_u, g.npm2);
-  const bool v0 = jj < g.ntm2 && e0 < g.nrm2;
-  const bool v1 = v0 && e0 + 1 < g.nrm2;
-  const bool south = v0 && jj == g.ntm2 - 1;
-  double rz = 0.0, s1a = 0.0, s1b = 0.0;
-  if (v0) {
-#pragma unroll 4
-    for (int kk = k0; kk < k1; kk++) {
-      const long long id = g.idx(e0, jj, kk);
-      float2 rv = *reinterpret_cast<const float2 *>(a.r + id);
-      if (KIND == U32_ITER) {
-        float2 xv = *reinterpret_cast<const float2 *>(a.xs + id);
-        const float2 pv = __ldg(reinterpret_cast<const float2 *>(a.p + id));
-        const float2 qv = __ldg(reinterpret_cast<const float2 *>(a.q + id));
-        xv.x = fmaf(alpha, pv.x, xv.x);
-        xv.y = fmaf(alpha, pv.y, xv.y);
-        rv.x = fmaf(-alpha, qv.x, rv.x);
-        rv.y = fmaf(-alpha, qv.y, rv.y);
-        *reinterpret_cast<float2 *>(a.xs + id) = xv;
-        *reinterpret_cast<float2 *>(a.r + id) = rv;
-      }
-      const float2 av = __ldg(reinterpret_cast<const float2 *>(a.ai + id));
-      const float zx = av.x * rv.x, zy = v1 ? av.y * rv.y : 0.0f;
-      rz = fma((double)rv.x, (double)zx, rz);
-      rz = fma((double)rv.y, (double)zy, rz);
-      if (south) {
-        const double wk = m.dph[kk + 2];
-        s1a += __dmul_rn((double)zx, wk) * m.pl_i;
-        s1b += __dmul_rn((double)zy, wk) * m.pl_i;
-      }
-    }
-  }
-  if (south) {
-    a.s1z_part[(long long)blockIdx.z * g.NRP + e0] = s1a;
-    a.s1z_part[(long long)blockIdx.z * g.NRP + e0 + 1] = v1 ? s1b : 0.0;
-  }
-  const double bs = block_sum<NTHR>(rz, red);
-  double total;
-  const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-  if (last_block_sum<NTHR>(bs, a.partials, &a.st->cnt_b, nb, &total, red)) {
-    if (threadIdx.x == 0) {
-      SolveState *s = a.st;
-      if (KIND == U32_ITER) {
-        s->rho_old = s->rho;
-        s->rho = total;
-        s->ncg = s->ncg + 1;
-        const double epssq = total / s->bdotb;
-        const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
-        s->epsn = epsn;
-        if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
-        if (!isfinite(epsn)) {
-          s->status = ST_BREAKDOWN;
-        } else if (epsn < s->epscg) {
-          s->status = ST_CONVERGED;  // candidate: confirmed by the FP64 residual
-        } else if (s->ncg >= s->ncgmax) {
-          s->status = ST_MAXIT;
-        }
-        s->beta = total / s->rho_old;
-      } else {
-        // restart from the true residual: rho <- r.z, beta continues the
-        // recurrence with the previous rho (zero on the first start).
-        s->rho = total;
-        s->beta = (s->rho_old > 0.0) ? total / s->rho_old : 0.0;
-        const double epssq = s->rho_true / s->bdotb;
-        const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
-        s->epsn = epsn;
-        if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
-        s->status = (epsn < s->epscg) ? ST_CONVERGED : (s->ncg >= s->ncgmax ? ST_MAXIT : ST_RUNNING);
-      }
-    }
-  }
-}
-
-// x += (double)xs; xs = 0   (the FP64 solution update of a reliable update)
-__global__ void k_fold(long long n, double *__restrict__ x, float *__restrict__ xs) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+  if (vs->status != ST_RUNNING) return;
+  const double alpha = vs->alpha;
+  const long long n4 = g.Np / 4;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4;
        t += (long long)gridDim.x * blockDim.x) {
-    x[t] += (double)xs[t];
-    xs[t] = 0.0f;
+    const long long id = 4 * t;
+    double2 x0 = *reinterpret_cast<const double2 *>(a.x + id);
+    double2 x1 = *reinterpret_cast<const double2 *>(a.x + id + 2);
+    const float4 pv = __ldg(reinterpret_cast<const float4 *>(a.p32 + id));
+    const float4 qv = __ldg(reinterpret_cast<const float4 *>(a.q32 + id));
+    float4 rv = *reinterpret_cast<const float4 *>(a.r32 + id);
+    x0.x = fma(alpha, (double)pv.x, x0.x);
+    x0.y = fma(alpha, (double)pv.y, x0.y);
+    x1.x = fma(alpha, (double)pv.z, x1.x);
+    x1.y = fma(alpha, (double)pv.w, x1.y);
+    rv.x = (float)fma(-alpha, (double)qv.x, (double)rv.x);
+    rv.y = (float)fma(-alpha, (double)qv.y, (double)rv.y);
+    rv.z = (float)fma(-alpha, (double)qv.z, (double)rv.z);
+    rv.w = (float)fma(-alpha, (double)qv.w, (double)rv.w);
+    *reinterpret_cast<double2 *>(a.x + id) = x0;
+    *reinterpret_cast<double2 *>(a.x + id + 2) = x1;
+    *reinterpret_cast<float4 *>(a.r32 + id) = rv;
   }
 }
 
-// r = b - q (FP64 true residual), r32 = (float)r, and r.(a_i r) in FP64.
-__global__ void __launch_bounds__(NTHR) k_true_resid(long long n, const double *__restrict__ b,
-                                                     const double *__restrict__ q, const float *__restrict__ ai,
-                                                     double *__restrict__ r, float *__restrict__ r32, SolveState *st,
-                                                     double *partials) {
-  __shared__ double red[NTHR / 32];
-  double acc = 0.0;
+// r = b - q (the FP64 true residual of a reliable update, q = A x) and its
+// FP32 copy for the inner iterations and the sweeps.
+__global__ void k_resid_cast(long long n, const double *__restrict__ b, const double *__restrict__ q,
+                             double *__restrict__ r, float *__restrict__ r32) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     const double v = b[t] - q[t];
     r[t] = v;
     r32[t] = (float)v;
-    acc = fma(v, (double)ai[t] * v, acc);
-  }
-  const double bs = block_sum<NTHR>(acc, red);
-  double total;
-  if (last_block_sum<NTHR>(bs, partials, &st->cnt_c, gridDim.x, &total, red)) {
-    if (threadIdx.x == 0) st->rho_true = total;
   }
 }
 
@@ -1138,6 +1085,8 @@ Solver::~Solver() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (dilu) dilu_destroy(this);
   if (graph32_exec) cudaGraphExecDestroy(graph32_exec);
+  if (evm0) cudaEventDestroy(evm0);
+  if (evm1) cudaEventDestroy(evm1);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   for (void *p : allocs) cudaFree(p);
@@ -1184,7 +1133,8 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   {
     int e;
     if ((e = set_stencil_smem<MODE_AX>()) || (e = set_stencil_smem<MODE_PCG>()) ||
-        (e = set_stencil_smem<MODE_PCGZ>()) || (e = set_stencil_smem<MODE_PCG32>()))
+        (e = set_stencil_smem<MODE_PCGZ>()) || (e = set_stencil_smem<MODE_PCG32>()) ||
+        (e = set_stencil_smem<MODE_PCGZ32>()))
       return e;
   }
   // k-chunking by a wave model: the grid is (i tiles, j tiles, k chunks);
@@ -1285,14 +1235,12 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
     if ((st = dilu_setup(this))) return st;
   }
   if (precision == POT3D_FP32_REFINED) {
-    if (ifprec == 2) {
-      pot3d_set_error("the FP32-refined solve supports ifprec 0 and 1");
-      return POT3D_ERR_ARG;
-    }
     const size_t fb = sizeof(float) * (size_t)g.Np;
-    if ((st = alloc((void **)&m_p32a, fb)) || (st = alloc((void **)&m_p32b, fb)) || (st = alloc((void **)&m_r32, fb)) ||
-        (st = alloc((void **)&m_q32, fb)) || (st = alloc((void **)&m_xs32, fb)))
+    if ((st = alloc((void **)&m_p32a, fb)) || (st = alloc((void **)&m_p32b, fb)) || (st = alloc((void **)&m_q32, fb)))
       return st;
+    if (ifprec != 2 && (st = alloc((void **)&m_r32, fb))) return st;  // ILU(0) uses the sweeps' r32
+    CK(cudaEventCreate(&evm0));
+    CK(cudaEventCreate(&evm1));
   }
   CK(cudaStreamSynchronize(stream));
   return POT3D_OK;
@@ -1670,65 +1618,91 @@ int Solver::energy_dev(const double *phi, double w[3]) {
 
 namespace pot3d {
 
-// One FP32 inner iteration: stencil+dot, update+dot.
+float *Solver::r32_inner() { return ifprec == 2 ? dilu_r32(this) : m_r32; }
+
+// One FP32-inner iteration.  Diagonal preconditioner: the PCG32 stencil
+// (p = beta p + a_i r, q = A p, p.q -> alpha) and the update (x += alpha p,
+// r -= alpha q, r.(a_i r) -> rho, beta, epsn).  ILU(0): the PCGZ32 stencil
+// (p = z + beta p), the x/r32 update, the two wavefront sweeps r32 -> z32,
+// and r.z -> rho, beta, epsn.
 int Solver::launch_iteration32() {
   dim3 grid(g.nit, g.njt, g.nkc);
   dim3 gridu(g.nit, g.njt, g.nkc_u);
   StencilArgs sa{};
-  sa.p_old32 = p32_cur;
   sa.p_new32 = p32_nxt;
-  sa.r32 = m_r32;
   sa.q32 = m_q32;
   sa.s1z_part = d_s1z;
   sa.s1p = d_s1p;
   sa.st = d_state;
   sa.partials = d_partials;
-  StencilMaps mp;
-  int stm;
-  if ((stm = tensor_map(p32_cur, false, &mp.m32[0])) || (stm = tensor_map(m_r32, false, &mp.m32[1])) ||
-      (stm = tensor_map(d_ai, false, &mp.m32[2])))
-    return stm;
-  mp.m64[0] = mp.m64[1] = mp.m32[0];
-  k_stencil<MODE_PCG32><<<grid, NTHR, StageLayout<MODE_PCG32>::smem, stream>>>(mp, g, m, sa);
-  Update32Args ua{};
-  ua.xs = m_xs32;
-  ua.p = p32_nxt;
-  ua.r = m_r32;
-  ua.q = m_q32;
+  UpdateArgs ua{};
+  ua.x = d_x;
+  ua.p32 = p32_nxt;
+  ua.q32 = m_q32;
+  ua.r32 = r32_inner();
   ua.ai = d_ai;
   ua.s1z_part = d_s1z;
   ua.st = d_state;
   ua.partials = d_partials;
-  k_update32<U32_ITER><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  StencilMaps mp;
+  int stm;
+  if ((stm = tensor_map(p32_cur, false, &mp.m32[0]))) return stm;
+  mp.m64[0] = mp.m64[1] = mp.m32[0];
+  if (ifprec == 2) {
+    if ((stm = tensor_map(dilu_z32(this), false, &mp.m32[1]))) return stm;
+    mp.m32[2] = mp.m32[0];
+    k_stencil<MODE_PCGZ32><<<grid, NTHR, StageLayout<MODE_PCGZ32>::smem, stream>>>(mp, g, m, sa);
+    const long long nb = std::min<long long>((g.Np / 4 + NTHR - 1) / NTHR, 148LL * 8);
+    k_update_x32<<<(int)nb, NTHR, 0, stream>>>(g, ua);
+    int st = dilu_sweeps(this, true);
+    if (st) return st;
+    ua.z32 = dilu_z32(this);
+    k_update<UPD_ZDOT, true, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  } else {
+    if ((stm = tensor_map(m_r32, false, &mp.m32[1])) || (stm = tensor_map(d_ai, false, &mp.m32[2]))) return stm;
+    k_stencil<MODE_PCG32><<<grid, NTHR, StageLayout<MODE_PCG32>::smem, stream>>>(mp, g, m, sa);
+    k_update<UPD_ITER, false, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  }
   std::swap(p32_cur, p32_nxt);
   return pot3d_cuda_status(cudaGetLastError(), "launch_iteration32");
 }
 
-// Reliable update: x += xs, r = b - A x in FP64, epsn of the true residual,
-// restart of the FP32 recurrence residual from it.
-int Solver::reliable_update(bool fold) {
+// Reliable update: r = b - A x in FP64 (and its FP32 copy), z = M^-1 r, and
+// rho = r.z with the reference's epsn of that residual (UPD_RU).
+int Solver::reliable_update() {
   int st;
-  if (fold) k_fold<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_x, m_xs32);
   if ((st = ax_padded(d_x, d_q))) return st;
-  k_true_resid<<<148 * 4, NTHR, 0, stream>>>(g.Np, d_b, d_q, d_ai, d_r, m_r32, d_state, d_partials + 4096);
+  k_resid_cast<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_b, d_q, d_r, r32_inner());
   dim3 gridu(g.nit, g.njt, g.nkc_u);
-  Update32Args ua{};
-  ua.xs = m_xs32;
-  ua.p = p32_cur;
-  ua.r = m_r32;
-  ua.q = m_q32;
+  UpdateArgs ua{};
+  ua.x = d_x;
+  ua.r = d_r;
   ua.ai = d_ai;
   ua.s1z_part = d_s1z;
   ua.st = d_state;
   ua.partials = d_partials;
-  k_update32<U32_RESTART><<<gridu, NTHR, 0, stream>>>(g, m, ua);
-  launches += (fold ? 1 : 0) + 4;
+  if (ifprec == 2) {
+    if ((st = dilu_sweeps(this, false))) return st;
+    ua.z32 = dilu_z32(this);
+    k_update<UPD_RU, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+    launches += 4 + sweep_launches();
+  } else {
+    k_update<UPD_RU, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+    launches += 4;
+  }
   return pot3d_cuda_status(cudaGetLastError(), "reliable_update");
 }
 
+// FP32-inner / FP64-refined PCG on d_x (guess) and d_b (RHS), the same
+// contract as cgsolve_padded.  Iterations run in CUDA graphs; between graphs
+// the host reads the device state and, when the recurrence's rho has fallen
+// by refine_ratio since the last reliable update or the recurrence reports
+// convergence (or ncgmax), makes a reliable update.  A reliable update whose
+// FP64 r.z fell by less than stall_drop is stagnant; stall_limit of them in
+// a row hand the solve to the FP64 PCG (cgsolve_padded) from the current x.
 int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info) {
-  (void)zero_guess;
   dim3 gridu(g.nit, g.njt, g.nkc_u);
+  const bool ilu = ifprec == 2;
   int st;
   SolveState s0{};
   s0.epscg = epscg;
@@ -1736,47 +1710,80 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   s0.hist = d_hist;
   s0.hist_cap = hist_cap;
   CK(cudaMemcpyAsync(d_state, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, stream));
-  CK(cudaEventRecord(ev0, stream));
+  CK(cudaEventRecord(evm0, stream));
   launches = 0;
+  last_fallback_iters = 0;
   p32_cur = m_p32a;
   p32_nxt = m_p32b;
   CK(cudaMemsetAsync(p32_cur, 0, sizeof(float) * g.Np, stream));
-  CK(cudaMemsetAsync(m_xs32, 0, sizeof(float) * g.Np, stream));
   CK(cudaMemsetAsync(d_s1p, 0, sizeof(double) * 2 * g.NRP, stream));
-  // bdotb = b . M^-1 b in FP64 (src/pot3d.F90:4293-4298)
   CK(cudaMemcpyAsync(d_r, d_b, sizeof(double) * g.Np, cudaMemcpyDeviceToDevice, stream));
-  UpdateArgs ub{};
-  ub.r = d_r;
-  ub.ai = d_ai;
-  ub.st = d_state;
-  ub.partials = d_partials;
-  k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, stream>>>(g, m, ub);
+  UpdateArgs ua{};
+  ua.x = d_x;
+  ua.r = d_r;
+  ua.ai = d_ai;
+  ua.s1z_part = d_s1z;
+  ua.st = d_state;
+  ua.partials = d_partials;
+  // bdotb = b . M^-1 b  (src/pot3d.F90:4293-4298); with ILU(0) this leaves
+  // r32 = (float)b and z32 = M^-1 b
+  k_cast_r32<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_r, r32_inner());
   launches += 1;
+  if (ilu) {
+    if ((st = dilu_reset(this))) return st;
+    if ((st = dilu_sweeps(this, false))) return st;
+    ua.z32 = dilu_z32(this);
+    k_update<UPD_BDOTB, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+    launches += 1 + sweep_launches();
+  } else {
+    k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+    launches += 1;
+  }
+  CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
-  if (h_state->bdotb == 0.0) {
+  if (h_state->bdotb == 0.0) {  // zero RHS -> zero solution (src/pot3d.F90:4302-4311)
     CK(cudaMemsetAsync(d_x, 0, sizeof(double) * g.Np, stream));
     CK(cudaStreamSynchronize(stream));
     *ierr = 0;
     last_ncg = 0;
     last_epsn = 0.0;
     last_seconds = 0.0;
+    last_refine = 0;
     if (info) memset(info, 0, sizeof(*info));
     return POT3D_OK;
   }
-  if ((st = reliable_update(false))) return st;
-  int n_refine = 0;
+  // initial residual r = b - A x in FP64, z = M^-1 r, rho (src/pot3d.F90:4317-4330)
+  if (!zero_guess) {
+    if ((st = ax_padded(d_x, d_q))) return st;
+    k_resid_cast<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_b, d_q, d_r, r32_inner());
+    launches += 3;
+    if (ilu) {
+      if ((st = dilu_sweeps(this, false))) return st;
+      launches += sweep_launches();
+    }
+  }
+  if (ilu)
+    k_update<UPD_INIT, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  else
+    k_update<UPD_INIT, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+  launches += 1;
+  CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
-  const double est_iter_s = 44.0 * (double)g.Np / 5.0e12 + 6e-6;
+
+  // Graphs of 2U iterations, at most 16: a reliable update is only made
+  // between graphs, and it must come before the recurrence has drifted far
+  // from the FP64 residual (small grids converge many decades per graph).
+  const double est_iter_s = (ilu ? 100.0 : 60.0) * (double)g.Np / 5.0e12 + 6e-6;
   int U = (int)std::ceil(0.5e-3 / est_iter_s);
-  U = std::max(2, std::min(U, 32));
+  U = std::max(1, std::min(U, 8));
   if (!graph32_exec || graph32_U != U) {
     if (graph32_exec) cudaGraphExecDestroy(graph32_exec);
     graph32_exec = nullptr;
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    for (int u = 0; u < 2 * U; u++) {
+    for (int u = 0; u < 2 * U; u++) {  // even count: the p ping-pong returns to m_p32a
       st = launch_iteration32();
       if (st) {
         cudaStreamEndCapture(stream, &graph);
@@ -1791,47 +1798,87 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
     graph32_U = U;
   }
   const long long per_graph = 2LL * U;
-  double rho_ref = h_state->rho;
-  int last_seen = -1, stalls = 0;
+  const long long nodes_per_iter = ilu ? 3 + sweep_launches() : 2;
+  double rho_ref = h_state->rho;  // r.z at the last FP64 residual
+  int ncg_ref = 0;                // iterations at the last FP64 residual
+  int n_refine = 0, stagnant = 0, stalls = 0;
+  bool fallback = false;
   while (h_state->status == ST_RUNNING) {
+    const int ncg0 = h_state->ncg;
     CK(cudaGraphLaunch(graph32_exec, stream));
-    launches += per_graph * 2;
+    launches += per_graph * nodes_per_iter;
     CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     const int status = h_state->status;
-    if (status == ST_BREAKDOWN) break;
-    const bool refresh = status == ST_CONVERGED || status == ST_MAXIT || h_state->rho < refine_ratio * rho_ref;
-    if (refresh) {
-      if ((st = reliable_update(true))) return st;
-      n_refine++;
-      CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
-      CK(cudaStreamSynchronize(stream));
-      rho_ref = h_state->rho;
-      if (status == ST_MAXIT && h_state->status == ST_RUNNING) h_state->status = ST_MAXIT;
-    }
-    if (h_state->ncg <= last_seen && h_state->status == ST_RUNNING) {
+    if (status == ST_BREAKDOWN || status == ST_TIMEOUT) break;
+    const int ran = h_state->ncg - ncg0;  // iterations of this graph (odd only if it stopped early)
+    if (ran <= 0) {
       if (++stalls >= 3) {
         pot3d_set_error("refined PCG state stopped advancing on the device");
         return POT3D_ERR_TIMEOUT;
       }
-    } else {
-      stalls = 0;
+      continue;
     }
-    last_seen = h_state->ncg;
+    stalls = 0;
+    // reliable update: convergence or ncgmax reported by the recurrence, its
+    // r.z fallen by refine_ratio or grown 100x since the last update (PCG's
+    // r.z is not monotone), or 1000 iterations without one
+    const bool refresh = status == ST_CONVERGED || status == ST_MAXIT || h_state->rho < refine_ratio * rho_ref ||
+                         h_state->rho > 100.0 * rho_ref || h_state->ncg - ncg_ref >= 1000;
+    if (!refresh) continue;
+    if ((st = reliable_update())) return st;
+    n_refine++;
+    CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (h_state->status != ST_RUNNING) break;
+    if (ran & 1) {
+      // the graph stopped after an odd number of iterations: the newest p is
+      // in the buffer the next graph writes first
+      CK(cudaMemcpyAsync(p32_cur, p32_nxt, sizeof(float) * g.Np, cudaMemcpyDeviceToDevice, stream));
+    }
+    // progress is judged over at least 10 iterations (updates that follow
+    // each other closely near convergence neither count nor reset)
+    if (h_state->ncg - ncg_ref >= 10) stagnant = (h_state->rho > stall_drop * rho_ref) ? stagnant + 1 : 0;
+    rho_ref = h_state->rho;
+    ncg_ref = h_state->ncg;
+    if (stagnant >= stall_limit) {
+      fallback = true;
+      break;
+    }
   }
-  CK(cudaEventRecord(ev1, stream));
+  int ncg_total = h_state->ncg;
+  int status = h_state->status;
+  double epsn = h_state->epsn;
+  if (fallback) {
+    // the FP32 recurrence stopped tracking the FP64 residual: plain FP64 PCG
+    // (same preconditioner) from the current x
+    const long long l0 = launches;
+    int ie = 1;
+    pot3d_solve_info_t inf2{};
+    if ((st = cgsolve_padded(false, std::max(1, ncgmax - ncg_total), epscg, &ie, &inf2))) return st;
+    launches = l0 + inf2.kernel_launches;
+    last_fallback_iters = std::max(1, inf2.ncg);
+    ncg_total += inf2.ncg;
+    status = ie == 0 ? ST_CONVERGED : ST_MAXIT;
+    epsn = inf2.epsn;
+  }
+  CK(cudaEventRecord(evm1, stream));
   CK(cudaStreamSynchronize(stream));
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, ev0, ev1);
-  last_ncg = h_state->ncg;
-  last_epsn = h_state->epsn;
+  cudaEventElapsedTime(&ms, evm0, evm1);
+  last_ncg = ncg_total;
+  last_epsn = epsn;
   last_seconds = ms * 1e-3;
   last_refine = n_refine;
-  if (h_state->status == ST_BREAKDOWN) {
-    pot3d_set_error("refined PCG breakdown (non-finite residual)");
+  if (status == ST_BREAKDOWN) {
+    pot3d_set_error("refined PCG breakdown (non-finite or zero curvature)");
     return POT3D_ERR_BREAKDOWN;
   }
-  *ierr = (h_state->status == ST_CONVERGED) ? 0 : 1;
+  if (status == ST_TIMEOUT) {
+    pot3d_set_error("a bounded device wait ran out in the refined PCG");
+    return POT3D_ERR_TIMEOUT;
+  }
+  *ierr = (status == ST_CONVERGED) ? 0 : 1;
   if (info) {
     info->ncg = last_ncg;
     info->n_refine = n_refine;

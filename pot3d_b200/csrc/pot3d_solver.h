@@ -39,14 +39,19 @@ struct Solver {
   float *d_ai = nullptr;        // diagonal preconditioner (FP32, padded)
   double *p_cur = nullptr, *p_nxt = nullptr;
 
-  // FP32-refined mode
-  float *m_p32a = nullptr, *m_p32b = nullptr, *m_r32 = nullptr, *m_q32 = nullptr, *m_xs32 = nullptr;
+  // FP32-inner / FP64-refined mode (both preconditioners)
+  float *m_p32a = nullptr, *m_p32b = nullptr, *m_r32 = nullptr, *m_q32 = nullptr;
   float *p32_cur = nullptr, *p32_nxt = nullptr;
   cudaGraphExec_t graph32_exec = nullptr;
   int graph32_U = 0;
-  double refine_ratio = 1e-4;  // reliable update when r.z fell by this factor
+  cudaEvent_t evm0 = nullptr, evm1 = nullptr;
+  double refine_ratio = 1e-4;  // reliable update once the recurrence's r.z fell by this factor
+  double stall_drop = 0.5;     // an update whose FP64 r.z fell by less than this factor is stagnant
+  int stall_limit = 2;         // consecutive stagnant updates that switch the solve to FP64 PCG
+  int last_fallback_iters = 0; // FP64 iterations after a switch in the last solve (0: none)
+  float *r32_inner();          // the FP32 recurrence residual (the sweeps' input with ILU(0))
   int launch_iteration32();
-  int reliable_update(bool fold);
+  int reliable_update();
   int mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info);
 
   cudaGraphExec_t graph_exec = nullptr;

@@ -87,6 +87,17 @@ class Pot3dSolver:
         self.last_info = info
         return ierr.value
 
+    def set_refine(self, refine_ratio: float = 1e-4, stall_drop: float = 0.5, stall_limit: int = 2):
+        """Reliable-update and stagnation controls of the FP32-refined solve."""
+        check(_lib.lib().pot3d_gpu_set_refine(self._h, refine_ratio, stall_drop, stall_limit))
+
+    def refine_info(self):
+        """(reliable updates, FP64 iterations after a switch to FP64 PCG) of
+        the last refined solve."""
+        nr, fb = C.c_int(0), C.c_int(0)
+        check(_lib.lib().pot3d_gpu_refine_info(self._h, C.byref(nr), C.byref(fb)))
+        return nr.value, fb.value
+
     def history(self, cap: int = 1 << 20) -> np.ndarray:
         """epsn after iterations 0..ncg of the last solve."""
         buf = np.zeros(cap)

@@ -148,3 +148,24 @@ def test_batch_specs_cover_the_uneven_grid_law():
     assert len({x[:3] for x in s}) > 4  # uneven
     assert all(2.0 <= x[3] <= 3.0 for x in s)
     assert len({x[4] for x in s}) == 48  # own Br seed per case
+
+
+@pytest.mark.parametrize("args", [(1, 15, 4, 91, 181), (2, 40, 20, 361, 721), (7, 5, 0, 13, 17),
+                                  (100, 40, 20, 91, 181)])
+def test_oracle_generator_matches_product_bitwise(args):
+    """The oracle's restatement of the seeded Br generator gives the product
+    generator's maps bit for bit, so the CPU reference arm can build the
+    workloads without the product library."""
+    a = O.synthetic_br(*args)
+    b = host.synthetic_br(*args)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_oracle_builds_the_bench_workload_bitwise():
+    w = host.WORKLOADS["pfss_63x91x181"]
+    m1, b1 = O.pfss_case(w["nr"], w["nt"], w["np"], w["lmax"], w["nbip"], w["seed"])
+    m2, b2 = host.pfss_case(w["nr"], w["nt"], w["np"], w["lmax"], w["nbip"], w["seed"])
+    assert np.array_equal(b1, b2)
+    for f in O.MESH_FIELDS:
+        assert np.array_equal(getattr(m1, f), getattr(m2, f))
