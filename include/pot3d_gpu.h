@@ -203,17 +203,18 @@ int pot3d_gpu_time_kernels(pot3d_gpu_solver *s, int reps, double ms[2], double b
 int pot3d_gpu_time_sweeps(pot3d_gpu_solver *s, int reps, double ms[2]);
 
 /* Magnetic energies like pot3d_gpu_energy, for callers that cannot allocate
- * device memory (their memory is owned by another allocator, or they run
- * while a stream is captured into a graph).  No counterpart in the
+ * device memory (their memory is owned by another allocator or pool, or
+ * their device footprint is fixed at start-up).  No counterpart in the
  * reference.  All arrays are caller-owned DEVICE arrays, 0-based, with the
  * lengths of pot3d_mesh_t; phi is (nr,nt,np) column-major; w receives
  * {W_r, W_t, W_p} on the device, asynchronously on `stream` (a cudaStream_t,
  * NULL for the default stream).  Scratch is a fixed file-scope device array
  * of 8192 phi planes (3 doubles each): np-2 > 8192 is rejected with
  * POT3D_ERR_ARG.  The library calls no cudaMalloc for it; the first call on
- * a device looks up the array's device address, so make it before any
- * stream capture.  Calls share that scratch: calls that overlap on the GPU
- * race and must be serialised by the caller. */
+ * a device looks up the array's device address and keeps it, so make it
+ * before any stream capture, and do not call again after cudaDeviceReset.
+ * Calls share that scratch: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 int pot3d_gpu_energy_noalloc(int nr, int nt, int np, const double *rh, const double *dr,
                              const double *drh, const double *dt, const double *dth,
                              const double *sth, const double *dp, const double *dph,

@@ -10,9 +10,11 @@
 //   z_i = (y_i - sum_{j in U(i)} a_ij z_j) * dinv_i  (rows descending)
 // with dinv_i = real(1/d_i in FP64, REAL32) (src/pot3d.F90:4706-4708).
 //
-// Nothing is stored but d and dinv: the FP32 couplings are the FP64
-// coefficients of load_matrix_pot3d_solve, formed on the fly in the
-// reference's operand order and rounded to FP32 as diacsr rounds them.
+// The factorisation stores d and dinv; the FP32 couplings are the FP64
+// coefficients of load_matrix_pot3d_solve formed in the reference's operand
+// order and rounded to FP32 as diacsr rounds them.  The wavefront sweeps
+// below read them (l = a/d forward, the upper a and dinv backward) from
+// streams formed once after the factorisation, in their tile-skewed order.
 // Every FP32 operation is an explicit __fdiv_rn/__fmul_rn/__fsub_rn so the
 // factor and both sweeps are bit-identical to the oracle.
 //
@@ -165,6 +167,7 @@ constexpr int WXR = 4;                  // exchange ring depth (chunks)
 constexpr int WAVE_BLOCK = WAVE_THREADS + 64;  // + exchange warp + copy warp
 constexpr unsigned WAVE_SPIN_LIMIT = 1u << 22;
 constexpr uint32_t WAVE_MBAR_LIMIT = 1u << 26;
+constexpr unsigned WAVE_POLL_NS = 32;        // exchange warp's sleep between polls of a face
 static_assert(WCH % WG == 0, "a chunk is whole stream groups");
 static_assert(WG * WPG > WSK + (WG - 1) + WG * WPD, "a plane group's slot is free when it is reissued");
 static_assert(WROUT >= WSK + 2 * WG + 2, "the copy warp stores a finished plane before its slot is needed again");
@@ -194,7 +197,10 @@ struct WaveArgs {
 
 __device__ __forceinline__ void wave_publish(unsigned long long *p, unsigned epoch, float v) {
   const unsigned long long w = ((unsigned long long)epoch << 32) | __float_as_uint(v);
-  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+  // no memory clobber: the word carries its own tag, so nothing has to be
+  // ordered around the store, and the compute warps' shared-memory traffic
+  // is not serialised behind it
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w));
 }
 __device__ __forceinline__ unsigned long long wave_load(const unsigned long long *p) {
   unsigned long long w;
@@ -301,7 +307,7 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
         S.abort = 1;
         break;
       }
-      __nanosleep(64);
+      __nanosleep(128);  // the ring is WXR chunks ahead: no hurry, and no issue slots taken
     }
     if (__any_sync(0xffffffffu, *(volatile int *)&S.abort != 0)) return;  // uniform over the warp
     bool ok = true;
@@ -342,7 +348,7 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
         ok = false;
         break;
       }
-      if (pit > 8) __nanosleep(32);
+      if (pit > 2) __nanosleep(WAVE_POLL_NS);
     }
     if (!ok) S.abort = 1;
     __syncwarp();
@@ -442,7 +448,9 @@ __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *
         *(volatile int *)&S.abort = 1;
         break;
       }
-      __nanosleep(20);
+      // the slots it refills are needed two groups (8 steps) later: a long
+      // sleep costs nothing there and leaves the issue slots to the compute warps
+      __nanosleep(128);
     }
   }
   if (*abort) {  // copies the compute warps may not wait for land before the block moves on
@@ -521,9 +529,9 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         }
         __threadfence_block();
       }
-      if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) return false;  // uniform over the compute warps
-      // the barrier that ended group gi-1 released its slots: tell the copy
-      // warp, which refills them
+      // the barrier that ended group gi-1 (which also decided, uniformly,
+      // that no thread had aborted) released its slots: tell the copy warp,
+      // which refills them
       if (T == 0) {
         __threadfence_block();
         *(volatile int *)&S.gdone = gi;
@@ -575,40 +583,56 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
             p_slot = p_slot + 1 == WPG ? 0 : p_slot + 1;
           }
         }
-        float y = 0.f;
+        // Branch-free step: a coupling the point does not have is applied as
+        // the product of a zero coefficient (the streams hold zeros there) and
+        // a finite operand (the neighbour value is zeroed by a select), which
+        // subtracts an exact zero; the terms keep lusol's order, so the
+        // values are lusol's (an exact-zero result may differ in its sign
+        // only).  With no branches the scheduler overlaps the point's own
+        // terms with the neighbour loads that follow the barrier.
         const int q = t - shift - sk;
-        if (valid && (unsigned)q < (unsigned)npm2) {
-          const int kk = FWD ? q : npm2 - 1 - q;
-          const float ne = ext_e ? ring[ring_e + uc * 16] : yprev[y_e];
-          const float nj = ext_j ? ring[ring_j + uc * 16] : yprev[y_j];
-          y = v_in;
-          if (FWD) {
-            // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1)
-            if (kk == npm2 - 1) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
-            if (kk > 0) y = __fsub_rn(y, __fmul_rn(k0, prev));
-            if (cpl_j) y = __fsub_rn(y, __fmul_rn(k1, nj));
-            if (cpl_e) y = __fsub_rn(y, __fmul_rn(k2, ne));
-            if (kk == 0) seam_y = y;
-          } else {
-            // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv
-            if (cpl_e) y = __fsub_rn(y, __fmul_rn(k0, ne));
-            if (cpl_j) y = __fsub_rn(y, __fmul_rn(k1, nj));
-            if (kk < npm2 - 1) y = __fsub_rn(y, __fmul_rn(k2, prev));
-            if (kk == 0) y = __fsub_rn(y, __fmul_rn(seam_c, seam_y));
-            y = __fmul_rn(y, k3);
-            if (kk == npm2 - 1) seam_y = y;
-          }
-          S.y[t & 1][jl][el] = y;
-          if constexpr (!FWD) S.zout[kk % WROUT][T] = y;
-          if (pub_e) wave_publish(xe_out + (size_t)t * 16, epoch, y);
-          if (pub_j) wave_publish(xj_out + (size_t)t * 16, epoch, y);
-          prev = y;
+        const bool act = valid && (unsigned)q < (unsigned)npm2;
+        const int kk = FWD ? q : npm2 - 1 - q;
+        const float *pe = ext_e ? ring + ring_e + uc * 16 : yprev + y_e;
+        const float *pj = ext_j ? ring + ring_j + uc * 16 : yprev + y_j;
+        const float ne = cpl_e ? *pe : 0.f;
+        const float nj = cpl_j ? *pj : 0.f;
+        float y;
+        if constexpr (FWD) {
+          // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1); l_k = 0 on the first plane
+          const float ks = kk == npm2 - 1 ? seam_c : 0.f;
+          y = __fsub_rn(__fsub_rn(v_in, __fmul_rn(ks, seam_y)), __fmul_rn(k0, prev));
+          y = __fsub_rn(y, __fmul_rn(k1, nj));
+          y = __fsub_rn(y, __fmul_rn(k2, ne));
+          y = act ? y : 0.f;
+          seam_y = (act && kk == 0) ? y : seam_y;
+        } else {
+          // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv; u_k = 0 on the last plane
+          const float ks = kk == 0 ? seam_c : 0.f;
+          y = __fsub_rn(v_in, __fmul_rn(k0, ne));
+          y = __fsub_rn(y, __fmul_rn(k1, nj));
+          y = __fsub_rn(y, __fmul_rn(k2, prev));
+          y = __fsub_rn(y, __fmul_rn(ks, seam_y));
+          y = __fmul_rn(y, k3);
+          y = act ? y : 0.f;
+          seam_y = (act && kk == npm2 - 1) ? y : seam_y;
+          if (act) S.zout[kk % WROUT][T] = y;
         }
+        S.y[t & 1][jl][el] = y;
+        if (pub_e && act) wave_publish(xe_out + (size_t)t * 16, epoch, y);
+        if (pub_j && act) wave_publish(xj_out + (size_t)t * 16, epoch, y);
+        prev = act ? y : prev;
         y4[u] = y;
         // backward: the group's z32 plane writes become visible to the copy
         // warp's TMA stores (async proxy) across the barrier and gdone
         if (!FWD && u == WG - 1) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        wave_bar_compute();
+        if (u == WG - 1) {
+          // the group's last barrier also ORs the abort flag, so every compute
+          // warp leaves at the same group when any wait gave up
+          if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) return false;
+        } else {
+          wave_bar_compute();
+        }
       }
       if constexpr (FWD) a.ys[((size_t)ti * G + gi) * WAVE_THREADS + T] = make_float4(y4[0], y4[1], y4[2], y4[3]);
     }

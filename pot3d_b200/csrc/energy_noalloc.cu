@@ -2,9 +2,8 @@
 //
 // Some callers cannot call cudaMalloc: a host program whose device memory is
 // owned by another allocator or pool (a Fortran/OpenMP runtime that maps all
-// arrays itself, a framework that forbids foreign allocations), code that
-// runs while a stream is being captured into a CUDA graph, or a process that
-// must not grow its device footprint after start-up.  For them this file
+// arrays itself, a framework that forbids foreign allocations), or a process
+// that must not grow its device footprint after start-up.  For them this file
 // provides pot3d_gpu_energy_noalloc: the same getb + magnetic_energy
 // reduction as pot3d_gpu_energy (src/pot3d.F90:6187-6321), on caller-owned
 // device arrays, with its scratch -- one partial sum per phi plane and
@@ -18,8 +17,10 @@
 // kernels overlap on the GPU (different streams, or different host threads)
 // race on it and must be serialised by the caller.  The first call on a
 // device looks up the array's device address with cudaGetSymbolAddress (the
-// host-side name is only a stand-in for it); make that first call before
-// any stream capture begins.
+// host-side name is only a stand-in for it) and keeps it for the life of the
+// process; make that first call before any stream capture begins, and do not
+// use the entry point again after cudaDeviceReset (the kept address belongs
+// to the context that looked it up).
 #include <cuda_runtime.h>
 
 #include <mutex>
