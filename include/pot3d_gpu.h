@@ -202,6 +202,15 @@ int pot3d_gpu_time_kernels(pot3d_gpu_solver *s, int reps, double ms[2], double b
  * calls, src/pot3d.F90 timing.out "PC"). */
 int pot3d_gpu_time_sweeps(pot3d_gpu_solver *s, int reps, double ms[2]);
 
+/* Failure-detection check of the ILU(0) wavefront sweeps (ifprec = 2): runs
+ * the forward sweep with one tile left undone, so the waits of the tiles
+ * that consume its faces cannot be satisfied and must give up after
+ * spin_limit polls (the library's own limit is 2^22).  Returns
+ * POT3D_ERR_TIMEOUT when they did; the device context stays usable and the
+ * next solve on the handle proceeds normally.  Nothing faults or hangs.  No
+ * counterpart in the reference, whose sweeps are sequential. */
+int pot3d_gpu_test_sweep_stall(pot3d_gpu_solver *s, unsigned spin_limit);
+
 /* Magnetic energies like pot3d_gpu_energy, for callers that cannot allocate
  * device memory (their memory is owned by another allocator or pool, or
  * their device footprint is fixed at start-up).  No counterpart in the

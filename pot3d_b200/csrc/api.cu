@@ -315,3 +315,13 @@ extern "C" int pot3d_gpu_refine_info(const pot3d_gpu_solver *h, int *n_refine, i
   if (fallback_iterations) *fallback_iterations = h->s.last_fallback_iters;
   return POT3D_OK;
 }
+
+extern "C" int pot3d_gpu_test_sweep_stall(pot3d_gpu_solver *h, unsigned spin_limit) {
+  int st;
+  if ((st = check_solver(h))) return st;
+  if (h->s.ifprec != 2 || spin_limit == 0) {
+    pot3d_set_error("pot3d_gpu_test_sweep_stall: needs ifprec 2 and a positive spin limit");
+    return POT3D_ERR_ARG;
+  }
+  return pot3d::dilu_test_stall(&h->s, spin_limit);
+}

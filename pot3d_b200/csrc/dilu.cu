@@ -191,6 +191,9 @@ struct WaveArgs {
   WaveCtl *ctl;
   SolveState *st;
   int check;             // skip when the solve state is no longer running
+  unsigned spin_limit;   // polls of a bounded wait before it gives up (WAVE_SPIN_LIMIT)
+  int stall_ticket;      // the block taking this ticket leaves its tile undone (-1: none); the
+                         // failure-detection test uses it to make its consumers' waits run out
   int nte, ntj, ntiles, ndiag, nsteps;
   int pad;               // nsteps - (npm2 + WSK): idle steps, trailing forward, leading backward
 };
@@ -303,7 +306,7 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
     // wait for a free ring slot (the compute warps consumed chunk c - WXR)
     unsigned it = 0;
     while (c - *(volatile int *)&S.consumed >= WXR && !*(volatile int *)&S.abort) {
-      if (++it > WAVE_SPIN_LIMIT) {
+      if (++it > a.spin_limit) {
         S.abort = 1;
         break;
       }
@@ -344,7 +347,7 @@ __device__ __forceinline__ void wave_exchange(const WaveArgs &a, typename WaveSm
         }
       }
       if (pub == NGC) break;
-      if (++pit > WAVE_SPIN_LIMIT) {
+      if (++pit > a.spin_limit) {
         ok = false;
         break;
       }
@@ -444,7 +447,7 @@ __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *
     if (worked) {
       it = 0;
     } else {
-      if (++it > WAVE_SPIN_LIMIT) {
+      if (++it > a.spin_limit) {
         *(volatile int *)&S.abort = 1;
         break;
       }
@@ -521,7 +524,7 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
       {  // wait until the exchange warp has step group gi in the ring
         unsigned it = 0;
         while (*(volatile int *)&S.ready <= gi && !*(volatile int *)&S.abort) {
-          if (++it > WAVE_SPIN_LIMIT) {
+          if (++it > a.spin_limit) {
             S.abort = 1;
             break;
           }
@@ -544,7 +547,7 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         const int need = WG * gi + WG - shift - WROUT;
         unsigned it = 0;
         while (*(volatile int *)&S.zflushed < need && !*(volatile int *)&S.abort) {
-          if (++it > WAVE_SPIN_LIMIT) {
+          if (++it > a.spin_limit) {
             S.abort = 1;
             break;
           }
@@ -666,7 +669,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
   while (run) {
     if (threadIdx.x == 0) {
       const unsigned t = atomicAdd(&a.ctl->ticket, 1u);
-      S.tile = t < (unsigned)a.ntiles ? a.order[FWD ? t : a.ntiles - 1 - t] : make_int2(-1, -1);
+      S.tile = (t < (unsigned)a.ntiles && (int)t != a.stall_ticket) ? a.order[FWD ? t : a.ntiles - 1 - t]
+                                                                    : make_int2(-1, -1);
       S.abort = 0;
       S.ready = 0;
       S.consumed = 0;
@@ -977,6 +981,8 @@ static WaveArgs wave_args(Solver *s, bool check) {
   a.ctl = D->ctl;
   a.st = s->d_state;
   a.check = check ? 1 : 0;
+  a.spin_limit = WAVE_SPIN_LIMIT;
+  a.stall_ticket = -1;
   a.nte = D->nte;
   a.ntj = D->ntj;
   a.ntiles = D->ntiles;
@@ -1178,6 +1184,27 @@ int dilu_time(Solver *s, int reps, double ms[2]) {
   }
   for (auto &x : e) cudaEventDestroy(x);
   return dilu_status(s);
+}
+
+// Failure-detection check: the forward sweep with the block that takes the
+// first ticket leaving its tile undone, so no face word of that tile is ever
+// published and every wait for one runs out after spin_limit polls.  Returns
+// the sweep's status (POT3D_ERR_TIMEOUT when the waits gave up as they must)
+// and leaves the sweeps reset for the next solve.
+int dilu_test_stall(Solver *s, unsigned spin_limit) {
+  DiluState *D = s->dilu;
+  int st;
+  if ((st = dilu_reset(s))) return st;
+  k_narrow_rhs<<<grid1d(s->g.Np), NTHR, 0, s->stream>>>(s->g.Np, s->d_b, D->r32);
+  WaveArgs a = wave_args(s, false);
+  a.spin_limit = spin_limit;
+  a.stall_ticket = 0;
+  k_dilu_wave<true><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_f, s->stream>>>(D->rmap, a);
+  if ((st = pot3d_cuda_status(cudaGetLastError(), "stalled sweep"))) return st;
+  const int sweep_status = dilu_status(s);
+  if ((st = dilu_reset(s))) return st;
+  CK(cudaStreamSynchronize(s->stream));
+  return sweep_status;
 }
 
 // Status of the sweeps issued so far (synchronises the solver stream).

@@ -101,6 +101,7 @@ int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, 
                       bool interior_only = false);
 int dilu_reset(Solver *s);
 int dilu_status(Solver *s);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
+int dilu_test_stall(Solver *s, unsigned spin_limit);  // a sweep whose waits must run out
 int dilu_time(Solver *s, int reps, double ms[2]);
 int dilu_diag(Solver *s, float *d_host, float *dinv_host);
 int dilu_sweep_launches(Solver *s);

@@ -57,6 +57,15 @@ class Pot3dSolver:
         self.close()
 
     # ---- reference-shaped API ------------------------------------------
+    def set_br0(self, br0):
+        """Replace the boundary map (nt, np), keeping mesh, operator and
+        preconditioner (set_flux for a new map)."""
+        b = np.asfortranarray(br0, dtype=np.float64)
+        if b.shape != (self.mesh.nt, self.mesh.np):
+            raise ValueError("br0 must have shape (nt, np)")
+        self._br0 = b
+        check(_lib.lib().pot3d_gpu_set_br0(self._h, dptr(b)))
+
     def rhs(self) -> np.ndarray:
         b = np.zeros(self.N)
         check(_lib.lib().pot3d_gpu_rhs(self._h, dptr(b)))
@@ -97,6 +106,12 @@ class Pot3dSolver:
         nr, fb = C.c_int(0), C.c_int(0)
         check(_lib.lib().pot3d_gpu_refine_info(self._h, C.byref(nr), C.byref(fb)))
         return nr.value, fb.value
+
+    def test_sweep_stall(self, spin_limit: int = 1 << 12) -> int:
+        """Status code of an ILU(0) forward sweep run with one tile left
+        undone (POT3D_ERR_TIMEOUT = 6 when its consumers' bounded waits gave
+        up); the solver stays usable."""
+        return int(_lib.lib().pot3d_gpu_test_sweep_stall(self._h, spin_limit))
 
     def history(self, cap: int = 1 << 20) -> np.ndarray:
         """epsn after iterations 0..ncg of the last solve."""
