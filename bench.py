@@ -289,6 +289,67 @@ def run_reference(args):
     return 0
 
 
+def run_legacy_lu(args):
+    """The legacy external-LU symbols (the -DCUSPARSE Fortran host's path,
+    src/lusol_cusparse.c:64,309,374) on the workload's diacsr CSR (built by
+    the oracle): wall time of load (factorisation) and of one application,
+    as the Fortran host sees them, and the application checked bit for bit
+    against the oracle's lusol.  The reference's own cuSPARSE shim is not
+    run (it crashed in this process: see the reason in the output)."""
+    import ctypes as C
+
+    import torch
+    O = _oracle()
+    w, opt, dnb = workload_params(args.workload)
+    mesh, br0 = oracle_case(args.workload, w["seed"], opt, dnb)
+    o = O.Solver(mesh, br0, option=opt, ifprec=1)
+    ia, ja, a = o.csr()
+    N = o.N
+    del o
+    rhs = np.random.default_rng(0).standard_normal(N)
+    out = {"workload": args.workload, "N": N, "nnz": int(ia[-1] - 1)}
+    z = {}
+    libs = {"ours": os.path.join(ROOT, "pot3d_b200", "libpot3d_gpu.so")}
+    out["reference_cusparse"] = {
+        "unavailable": "the reference's src/lusol_cusparse.c, built against the image's cuSPARSE and driven with "
+                       "this CSR from a torch process, crashed the process (SIGSEGV in load_external_lu_solver); "
+                       "not run again"}
+    for name, path in libs.items():
+        L = C.CDLL(path)  # RTLD_LOCAL: each library's symbols resolve on its own handle
+        L.load_external_lu_solver.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.external_lu_solver.argtypes = [C.c_void_p]
+        ia_d = torch.tensor(ia, dtype=torch.int32, device="cuda")
+        ja_d = torch.tensor(ja, dtype=torch.int32, device="cuda")
+        a_d = torch.tensor(a, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.load_external_lu_solver(a_d.data_ptr(), ia_d.data_ptr(), ja_d.data_ptr(), N, int(ia[-1]))
+        torch.cuda.synchronize()
+        t_load = time.perf_counter() - t0
+        x = torch.tensor(rhs, device="cuda")
+        L.external_lu_solver(x.data_ptr())
+        torch.cuda.synchronize()
+        z[name] = x.cpu().numpy()
+        ts = []
+        for _ in range(args.warmup + args.steps):
+            x.copy_(torch.tensor(rhs, device="cuda"))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            L.external_lu_solver(x.data_ptr())
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        L.unload_external_lu_solver()
+        out[name] = {"load_s": t_load, "apply_ms": 1e3 * float(np.mean(ts[args.warmup:])),
+                     "apply_ms_min": 1e3 * float(np.min(ts[args.warmup:]))}
+        del ia_d, ja_d, a_d, x
+    if N <= 2_000_000:  # the oracle's lusol on the host: bit for bit
+        o = O.Solver(mesh, br0, option=opt, ifprec=2)
+        out["ours"]["bitwise_vs_oracle_lusol"] = bool(np.array_equal(z["ours"], o.prec(rhs)))
+        del o
+    print(json.dumps({"legacy_lu": out}), flush=True)
+    return 0
+
+
 def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
@@ -315,6 +376,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the FP64 solves timed beside the headline solve")
     ap.add_argument("--no-parity", action="store_true", help="skip the 1e-11 parity solves")
+    ap.add_argument("--legacy-lu", action="store_true",
+                    help="time the legacy external-LU symbols against the reference's cuSPARSE shim and exit")
     ap.add_argument("--kernel-timing-only", action="store_true",
                     help="time the hot kernels briefly (stencil and update, or with --ifprec 2 the two "
                          "ILU(0) sweeps; used for ncu captures) and exit")
@@ -324,6 +387,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args)
+    if args.legacy_lu:
+        return run_legacy_lu(args)
 
     ws, rank, local = dist_init()
     import torch
@@ -493,13 +558,18 @@ def main():
                   "timed_1e-9_phi_rel_l2": rel_l2(phi9, phi64),
                   "timed_1e-9_energy_rel_err": float(np.max(np.abs(w9 - w64) / np.abs(w64))),
                   "energies_1e-11": w11.tolist()}
-        fix = oracle_fixture(args.workload, 1) if rank == 0 else None
-        if fix is not None:
+        parity["oracle"] = {}
+        for pf in (2, 1):
+            fix = oracle_fixture(args.workload, pf) if rank == 0 else None
+            if fix is None:
+                continue
             wo = np.asarray(fix["energy"])
             sl = np.stack([phi11[i - 1, ::fix["stride"], ::fix["stride"]] for i in fix["slice_i"]])
-            parity["oracle"] = {"source": f"tests/golden/{args.workload}_oracle_ifprec1 (oracle FP64 PCG to 1e-11)",
-                                "energy_rel_err": float(np.max(np.abs(w11 - wo) / np.abs(wo))),
-                                "phi_slices_rel_l2": rel_l2(sl, fix["phi_slices"])}
+            parity["oracle"][f"ifprec{pf}"] = {
+                "source": f"tests/golden/{args.workload}_oracle_ifprec{pf} (oracle FP64 PCG to 1e-11, "
+                          f"{fix['iterations']} iterations)",
+                "energy_rel_err": float(np.max(np.abs(w11 - wo) / np.abs(wo))),
+                "phi_slices_rel_l2": rel_l2(sl, fix["phi_slices"])}
     if s64 is not None:
         s64.close()
 

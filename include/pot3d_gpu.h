@@ -127,6 +127,19 @@ long pot3d_gpu_size(const pot3d_gpu_solver *s);
  * solves one map per run. */
 int pot3d_gpu_set_br0(pot3d_gpu_solver *s, const double *br0);
 
+/* readbr after the file read (src/pot3d.F90:6751-6829) and set_flux's |Br|
+ * for 'open' (src/pot3d.F90:3832), on the device: the map fi(ntn,npn)
+ * (host, column-major) with its increasing scales tn (theta, ntn) and pn
+ * (phi, npn) is interpolated bilinearly onto th(2:ntm1) x ph(2:npm1), copied
+ * periodically, given the m=0 pole rows and flux-balanced unless
+ * do_not_balance_flux ('ss'/'open'); option 0 'potential', 1 'open', 2 'ss'.
+ * The result replaces the solve's br0 (and its RHS, as pot3d_gpu_set_br0);
+ * br0_out (host, (nt,np)) receives it when non-NULL.  Bit for bit the host
+ * readbr of include/pot3d_host.h.  Returns POT3D_ERR_ARG for scales that do
+ * not increase or a mesh point outside them. */
+int pot3d_gpu_br0_from_map(pot3d_gpu_solver *s, int ntn, int npn, const double *tn, const double *pn,
+                           const double *fi, int option, int do_not_balance_flux, double *br0_out);
+
 /* RHS by potfld's boundary trick, src/pot3d.F90:3937-3950 (host output). */
 int pot3d_gpu_rhs(pot3d_gpu_solver *s, double *rhs);
 
@@ -243,11 +256,26 @@ int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const double *cons
  * cases by one wavefront kernel per direction). */
 int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
                               const double *pm_r1s, int tk, int ifprec, pot3d_gpu_batch **out);
+/* The same with the arithmetic chosen as well: precision POT3D_FP32_REFINED
+ * runs every case's inner iterations in FP32 storage (the batched forms of
+ * the single solve's refined kernels) with per-case FP64 reliable updates,
+ * per-case stagnation switches to FP64 PCG and per-case convergence on the
+ * FP64 residual, as pot3d_gpu_set_refine describes for one case. */
+int pot3d_gpu_batch_create_mode(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                                const double *pm_r1s, int tk, int ifprec, int precision,
+                                pot3d_gpu_batch **out);
+/* Initial guess of case i for the following pot3d_gpu_batch_solve calls
+ * (host, packed layout of length N_i, copied; NULL returns to x = 0), as
+ * potfld's x_cg = 0 (src/pot3d.F90:3924) replaced by, e.g., a learned
+ * prediction.  PCG from the guess decides convergence as from zero. */
+int pot3d_gpu_batch_set_guess(pot3d_gpu_batch *b, int i, const double *x);
 /* Autotuner: times `iters` batched iterations for each candidate planes per
  * block, keeps the fastest (*best_tk; ms_out[c] = time of candidate c). */
 int pot3d_gpu_batch_tune(pot3d_gpu_batch *b, const int *candidates, int ncand, int iters, int *best_tk,
                          float *ms_out);
-/* Solve all cases from x = 0 to epscg (ernorm's rule per case); ierr[i],
+/* Solve all cases from their guesses (x = 0 unless set) to epscg (ernorm's
+ * rule per case; with FP32_REFINED, info[i].n_refine the case's reliable
+ * updates); ierr[i],
  * info[i] per case; *seconds = device time of the whole batch. */
 int pot3d_gpu_batch_solve(pot3d_gpu_batch *b, int ncgmax, double epscg, int *ierr,
                           pot3d_solve_info_t *info, double *seconds);

@@ -2,16 +2,20 @@
 
 The workload: n independent PFSS cases, each with its own grid drawn from
 nr in {63, 95, 127}, nt in {91, 181}, np in {181, 361}, its own seeded Br map
-(harmonics l <= 15, 4 bipoles) and its own source-surface radius r1 drawn
+(harmonics l <= 40, 20 bipoles) and its own source-surface radius r1 drawn
 uniformly from [2, 3]; all are solved to the same ernorm tolerance by one
 BatchSolver, whose kernels cover every unfinished case per launch.
 
-    python -m pot3d_b200.batch [--n 48] [--seed 0] [--epscg 1e-9] [--ifprec 1|2] [--out f.json]
+    python -m pot3d_b200.batch [--n 48] [--seed 0] [--epscg 1e-9] [--ifprec 1|2]
+                               [--precision fp32_refined|fp64] [--out f.json]
 
-reports the batch time, per-case iterations, the autotuner's choice and the
-aggregate algorithmic HBM throughput (per unknown and iteration 80 bytes
-with the diagonal preconditioner, 136 with ILU(0)), and compares with
-the same cases solved one after another by the single-case solver.
+reports the batch time, per-case iterations and reliable updates, the
+autotuner's choice and the aggregate algorithmic HBM throughput (bytes per
+unknown and iteration: FP64 80 with the diagonal preconditioner and 104 with
+ILU(0), FP32-inner 40 and 64), and compares with the same cases solved one
+after another by the single-case solver in the same arithmetic.  The
+default is the configuration's form: ILU(0), FP32-inner iterations with
+FP64 reliable updates, per-case convergence.
 """
 from __future__ import annotations
 
@@ -27,7 +31,9 @@ from .host import PM_R1
 NR = (63, 95, 127)
 NT = (91, 181)
 NP = (181, 361)
-BYTES_PER_UNKNOWN_ITER = {1: 80.0, 2: 136.0}
+LMAX, NBIP = 40, 20  # the batch's map generator: harmonics l <= 40 and 20 bipoles
+BYTES_PER_UNKNOWN_ITER = {("fp64", 1): 80.0, ("fp64", 2): 104.0, ("fp32_refined", 1): 40.0,
+                          ("fp32_refined", 2): 64.0}
 
 
 def batch_specs(n: int = 48, seed: int = 0):
@@ -44,7 +50,7 @@ def batch_cases(specs):
     """Meshes and br0 maps of the specs (PFSS grid law, source surface)."""
     meshes, brs = [], []
     for nr, nt, np_, r1, s in specs:
-        mesh, br0 = host.pfss_case(nr, nt, np_, 15, 4, s, r1=r1)
+        mesh, br0 = host.pfss_case(nr, nt, np_, LMAX, NBIP, s, r1=r1)
         meshes.append(mesh)
         brs.append(br0)
     return meshes, brs
@@ -59,13 +65,15 @@ def main(argv=None):
     ap.add_argument("--no-sequential", action="store_true")
     ap.add_argument("--repeats", type=int, default=2)
     ap.add_argument("--out", default=None)
-    ap.add_argument("--ifprec", type=int, default=1, help="1: diagonal, 2: ILU(0) (batched wavefront sweeps)")
+    ap.add_argument("--ifprec", type=int, default=2, help="1: diagonal, 2: ILU(0) (batched wavefront sweeps)")
+    ap.add_argument("--precision", default="fp32_refined", choices=["fp32_refined", "fp64"])
     a = ap.parse_args(argv)
     specs = batch_specs(a.n, a.seed)
     meshes, brs = batch_cases(specs)
     unknowns = [(m.nr - 2) * (m.nt - 2) * (m.np - 2) for m in meshes]
-    rep = {"n": a.n, "seed": a.seed, "epscg": a.epscg, "ifprec": a.ifprec, "specs": specs}
-    with BatchSolver(meshes, brs, [PM_R1["ss"]] * a.n, ifprec=a.ifprec) as b:
+    rep = {"n": a.n, "seed": a.seed, "epscg": a.epscg, "ifprec": a.ifprec, "precision": a.precision,
+           "map": {"lmax": LMAX, "bipoles": NBIP}, "specs": specs}
+    with BatchSolver(meshes, brs, [PM_R1["ss"]] * a.n, ifprec=a.ifprec, precision=a.precision) as b:
         t0 = time.perf_counter()
         best, times = b.tune()
         rep["tune"] = {"best_planes_per_block": best, "ms": times, "seconds": time.perf_counter() - t0}
@@ -75,8 +83,9 @@ def main(argv=None):
             secs.append(b.seconds)
         ncg = [i.ncg for i in b.infos]
         rep["batch"] = {"seconds": min(secs), "all_seconds": secs, "ierr": ierr, "ncg": ncg,
+                        "reliable_updates": [i.n_refine for i in b.infos],
                         "kernel_launches": b.infos[0].kernel_launches}
-        bpu = BYTES_PER_UNKNOWN_ITER[a.ifprec]
+        bpu = BYTES_PER_UNKNOWN_ITER[(a.precision, a.ifprec)]
         moved = sum(bpu * u * k for u, k in zip(unknowns, ncg))
         rep["batch"]["algorithmic_gbs"] = moved / min(secs) / 1e9
         rep["batch"]["max_case_iterations"] = max(ncg)
@@ -84,7 +93,7 @@ def main(argv=None):
     if not a.no_sequential:
         tot, ncg1 = 0.0, []
         for q, (m, br) in enumerate(zip(meshes, brs)):
-            with Pot3dSolver(m, br, ifprec=a.ifprec) as s:
+            with Pot3dSolver(m, br, ifprec=a.ifprec, precision=a.precision) as s:
                 best_t = None
                 for _ in range(a.repeats):
                     x = np.zeros(s.N)

@@ -325,3 +325,7 @@ extern "C" int pot3d_gpu_test_sweep_stall(pot3d_gpu_solver *h, unsigned spin_lim
   }
   return pot3d::dilu_test_stall(&h->s, spin_limit);
 }
+
+namespace pot3d {
+Solver *solver_of(pot3d_gpu_solver *h) { return &h->s; }
+}  // namespace pot3d

@@ -844,6 +844,82 @@ __global__ void k_wave_streams(Geo g, DevMesh m, const float *__restrict__ d, co
   }
 }
 
+// The same streams from a factored 1-based CSR with POT3D's 7-point pattern
+// (the route of load_external_lu_solver for such a matrix): each row's L
+// entries as ilu0 left them (a_ik / d_k) and its upper entries, found by
+// their column offsets, and dinv; zero where a thread has no point at a step
+// or the row has no such coupling.  The values are the ones k_wave_streams
+// forms from the mesh, since the CSR holds the same FP32 coefficients.
+__global__ void k_wave_streams_csr(Geo g, const int *__restrict__ ia, const int *__restrict__ ja,
+                                   const int *__restrict__ dptr, const float *__restrict__ a,
+                                   const float *__restrict__ dinv, int nte, int ntiles, int nsteps, int pad,
+                                   float4 *__restrict__ lf, float4 *__restrict__ ub) {
+  const int G = nsteps / WG;
+  const long long P = (long long)g.nrm2 * g.ntm2;
+  const long long total = (long long)ntiles * G * WAVE_THREADS;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int T = (int)(q % WAVE_THREADS);
+    const long long rr = q / WAVE_THREADS;
+    const int gi = (int)(rr % G);
+    const int ti = (int)(rr / G);
+    const int te = ti % nte, tj = ti / nte;
+    const int el = T & (WE - 1), jl = T / WE;
+    const int e = te * WE + el, jj = tj * WJT + jl;
+    const bool valid = e < g.nrm2 && jj < g.ntm2;
+    float l[3][WG] = {}, u[4][WG] = {};
+    for (int s = 0; s < WG; s++) {
+      const int t = gi * WG + s;
+      const int kf = t - (el + jl);
+      if (valid && kf >= 0 && kf < g.npm2) {  // forward row (e, jj, kf)
+        const long long i = ((long long)kf * g.ntm2 + jj) * g.nrm2 + e;
+        for (int k = ia[i] - 1; k < dptr[i]; k++) {
+          const long long c = ja[k] - 1;
+          if (c == i - P) l[0][s] = a[k];
+          else if (c == i - g.nrm2) l[1][s] = a[k];
+          else if (c == i - 1) l[2][s] = a[k];
+        }
+      }
+      const int qb = t - pad - ((WE - 1 - el) + (WJT - 1 - jl));
+      if (valid && qb >= 0 && qb < g.npm2) {  // backward row (e, jj, npm2-1-qb)
+        const int kb = g.npm2 - 1 - qb;
+        const long long i = ((long long)kb * g.ntm2 + jj) * g.nrm2 + e;
+        for (int k = dptr[i] + 1; k < ia[i + 1] - 1; k++) {
+          const long long c = ja[k] - 1;
+          if (c == i + 1) u[0][s] = a[k];
+          else if (c == i + g.nrm2) u[1][s] = a[k];
+          else if (c == i + P) u[2][s] = a[k];
+        }
+        u[3][s] = dinv[i];
+      }
+    }
+    const size_t base = (size_t)ti * G + gi;
+    for (int c = 0; c < 3; c++) lf[(base * 3 + c) * WAVE_THREADS + T] = make_float4(l[c][0], l[c][1], l[c][2], l[c][3]);
+    for (int c = 0; c < 4; c++) ub[(base * 4 + c) * WAVE_THREADS + T] = make_float4(u[c][0], u[c][1], u[c][2], u[c][3]);
+  }
+}
+
+// Seam couplings from the CSR: the last plane's L entry to the first plane
+// (its smallest column) and the first plane's U entry to the last (largest).
+__global__ void k_wave_seam_csr(Geo g, const int *__restrict__ ia, const int *__restrict__ ja,
+                                const int *__restrict__ dptr, const float *__restrict__ a, float *__restrict__ seam_f,
+                                float *__restrict__ seam_b) {
+  const long long n = (long long)g.ntm2 * g.nrm2, P = n, W = (long long)(g.npm2 - 1) * P;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(q % g.nrm2), jj = (int)(q / g.nrm2);
+    const long long row = (long long)jj * g.NRP + e;
+    const long long il = W + q, i0 = q;  // the line's last and first plane rows
+    float sf = 0.f, sb = 0.f;
+    for (int k = ia[il] - 1; k < dptr[il]; k++)
+      if (ja[k] - 1 == il - W) sf = a[k];
+    for (int k = dptr[i0] + 1; k < ia[i0 + 1] - 1; k++)
+      if (ja[k] - 1 == i0 + W) sb = a[k];
+    seam_f[row] = sf;
+    seam_b[row] = sb;
+  }
+}
+
 // Per-line seam coefficients: forward a7/d(e, j, 0) of the last plane,
 // backward a1 of the first plane.
 __global__ void k_wave_seam(Geo g, DevMesh m, const float *__restrict__ d, float *__restrict__ seam_f,
@@ -1142,6 +1218,24 @@ int dilu_setup(Solver *s) {
                                                    D->nsteps - (g.npm2 + WSK), D->lf, D->ub);
   k_wave_seam<<<grid1d((long long)g.ntm2 * g.nrm2), NTHR, 0, s->stream>>>(g, s->m, D->d, D->seam_f, D->seam_b);
   return pot3d_cuda_status(cudaGetLastError(), "sweep coefficient streams");
+}
+
+// Wavefront sweeps for a caller's factored CSR with the 7-point pattern of a
+// nrm2 x ntm2 x npm2 interior (load_external_lu_solver's route): s carries
+// only the grid and a stream; the streams come from the CSR (device arrays).
+int dilu_setup_csr(Solver *s, const int *ia, const int *ja, const int *dptr, const float *a, const float *dinv) {
+  const Geo &g = s->g;
+  s->dilu = new DiluState();
+  DiluState *D = s->dilu;
+  int st;
+  const size_t fb = sizeof(float) * (size_t)g.Np;
+  if ((st = s->alloc((void **)&D->r32, fb)) || (st = s->alloc((void **)&D->z32, fb))) return st;
+  if ((st = wave_setup(s))) return st;
+  k_wave_streams_csr<<<148 * 8, NTHR, 0, s->stream>>>(g, ia, ja, dptr, a, dinv, D->nte, D->ntiles, D->nsteps,
+                                                      D->nsteps - (g.npm2 + WSK), D->lf, D->ub);
+  k_wave_seam_csr<<<grid1d((long long)g.ntm2 * g.nrm2), NTHR, 0, s->stream>>>(g, ia, ja, dptr, a, D->seam_f,
+                                                                             D->seam_b);
+  return pot3d_cuda_status(cudaGetLastError(), "sweep streams from the CSR");
 }
 
 void dilu_destroy(Solver *s) {

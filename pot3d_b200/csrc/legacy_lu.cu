@@ -16,8 +16,13 @@
 // (src/pot3d.F90:4706-4708).
 //
 // The sparsity analysis (row levels of L and of U) runs once on the host
-// from the integer structure; factorisation and sweeps are one kernel per
-// level, and the per-call sweep sequence is replayed as a CUDA graph.
+// from the integer structure and the factorisation is one kernel per level.
+// When the matrix has the 7-point pattern diacsr builds for a
+// nrm2 x ntm2 x npm2 interior (src/pot3d.F90:4870-5018: boundary couplings
+// dropped, the periodic phi seam kept) -- recognised from the columns alone --
+// each call runs the two wavefront sweeps of the whole-solve path, their
+// coefficient streams formed from the factored CSR; any other pattern runs
+// level-scheduled sweeps (one kernel per level) replayed as a CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +32,7 @@
 #include <vector>
 
 #include "pot3d_internal.cuh"
+#include "pot3d_solver.h"
 
 namespace {
 
@@ -41,10 +47,63 @@ struct LegacyLU {
   int *rows_f = nullptr, *rows_b = nullptr;  // rows ordered by level
   std::vector<int> lev_f, lev_b;             // level offsets into rows_*
   cudaStream_t stream = nullptr;
-  cudaGraphExec_t sweeps = nullptr;
+  cudaGraphExec_t sweeps = nullptr;   // level-scheduled route
+  pot3d::Solver *wave = nullptr;      // wavefront route (7-point pattern): grid, stream, sweeps
   bool loaded = false;
 };
 LegacyLU g_lu;
+
+// The grid of a CSR with diacsr's 7-point pattern, or false.  Row 0 gives
+// the column offsets nrm2 (j+1) and nrm2*ntm2 (k+1); every row must then hold
+// exactly the columns diacsr writes for its (e, j, k), in ascending order.
+bool seven_point(int N, const std::vector<int> &ia, const std::vector<int> &ja, int *nrm2_, int *ntm2_,
+                 int *npm2_) {
+  if (N < 36 || ia[1] - ia[0] != 5) return false;
+  const int c1 = ja[ia[0]], cj = ja[ia[0] + 1] - 1, ck = ja[ia[0] + 2] - 1;
+  if (ja[ia[0] - 1] != 1 || c1 != 2 || cj < 3 || ck <= cj || ck % cj != 0 || N % ck != 0) return false;
+  const long long nrm2 = cj, P = ck, ntm2 = P / nrm2, npm2 = N / P;
+  if (nrm2 < 3 || ntm2 < 3 || npm2 < 4) return false;
+  const long long W = (npm2 - 1) * P;
+  std::vector<long long> want;
+  for (long long i = 0; i < N; i++) {
+    const long long e = i % nrm2, j = (i / nrm2) % ntm2, k = i / P;
+    want.clear();
+    if (k == npm2 - 1) want.push_back(i - W);
+    if (k > 0) want.push_back(i - P);
+    if (j > 0) want.push_back(i - nrm2);
+    if (e > 0) want.push_back(i - 1);
+    want.push_back(i);
+    if (e < nrm2 - 1) want.push_back(i + 1);
+    if (j < ntm2 - 1) want.push_back(i + nrm2);
+    if (k < npm2 - 1) want.push_back(i + P);
+    if (k == 0) want.push_back(i + W);
+    if (ia[i + 1] - ia[i] != (int)want.size()) return false;
+    for (size_t q = 0; q < want.size(); q++)
+      if (ja[ia[i] - 1 + q] - 1 != want[q]) return false;
+  }
+  *nrm2_ = (int)nrm2;
+  *ntm2_ = (int)ntm2;
+  *npm2_ = (int)npm2;
+  return true;
+}
+
+// Packed FP64 vector -> padded FP32 sweep input, and back.
+__global__ void k_lu_narrow_pad(pot3d::Geo g, const double *__restrict__ x, float *__restrict__ r32) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.N;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(t % g.nrm2);
+    const long long line = t / g.nrm2;
+    r32[line * g.NRP + e] = (float)x[t];
+  }
+}
+__global__ void k_lu_widen_pad(pot3d::Geo g, const float *__restrict__ z32, double *__restrict__ x) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.N;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(t % g.nrm2);
+    const long long line = t / g.nrm2;
+    x[t] = (double)z32[line * g.NRP + e];
+  }
+}
 
 [[noreturn]] void die(const char *what, const char *detail) {
   printf(" ERROR! %s %s \n", what, detail ? detail : "");
@@ -195,6 +254,28 @@ extern "C" void load_external_lu_solver(float *CSR_LU, int *CSR_I, int *CSR_J, i
   ck(cudaStreamSynchronize(L.stream), "ILU0 Factorization Error =");
   cudaFree(d_piv);
   if (piv != big) die("ILU0 Zero Pivot at row", std::to_string(piv).c_str());
+  int nrm2 = 0, ntm2 = 0, npm2 = 0;
+  if (seven_point(N, ia, ja, &nrm2, &ntm2, &npm2)) {
+    // the wavefront route: a solver object holding only the grid and a stream
+    pot3d::Solver *w = new pot3d::Solver();
+    pot3d::Geo &g = w->g;
+    g.nrm2 = nrm2;
+    g.ntm2 = ntm2;
+    g.npm2 = npm2;
+    g.nr = nrm2 + 2;
+    g.nt = ntm2 + 2;
+    g.np = npm2 + 2;
+    g.NRP = (nrm2 + 15) / 16 * 16;
+    g.N = (long long)nrm2 * ntm2 * npm2;
+    g.Np = (long long)g.NRP * ntm2 * npm2;
+    L.wave = w;
+    ck(cudaStreamCreate(&w->stream), "ILU0 Setup Error =");
+    if (pot3d::dilu_setup_csr(w, L.ia, L.ja, L.dptr, L.val, L.dinv) != POT3D_OK)
+      die("ILU0 Setup Error =", pot3d_gpu_last_error());
+    ck(cudaStreamSynchronize(w->stream), "ILU0 Setup Error =");
+    L.loaded = true;
+    return;
+  }
   // The per-call sweeps, captured once.
   cudaGraph_t graph;
   ck(cudaStreamBeginCapture(L.stream, cudaStreamCaptureModeThreadLocal), "Forward Solve Error =");
@@ -220,6 +301,16 @@ extern "C" void external_lu_solver(double *x) {
   LegacyLU &L = g_lu;
   if (!L.loaded) die("Forward Solve Error =", "load_external_lu_solver was not called");
   const int nb = std::min((L.N + 255) / 256, 148 * 8);
+  if (L.wave) {
+    pot3d::Solver *w = L.wave;
+    k_lu_narrow_pad<<<nb, 256, 0, w->stream>>>(w->g, x, pot3d::dilu_r32(w));
+    ck(cudaGetLastError(), "Forward Solve Error =");
+    if (pot3d::dilu_sweeps(w, false) != POT3D_OK) die("Forward Solve Error =", pot3d_gpu_last_error());
+    k_lu_widen_pad<<<nb, 256, 0, w->stream>>>(w->g, pot3d::dilu_z32(w), x);
+    ck(cudaGetLastError(), "Backward Solve Error =");
+    if (pot3d::dilu_status(w) != POT3D_OK) die("Backward Solve Error =", pot3d_gpu_last_error());
+    return;
+  }
   k_lu_narrow<<<nb, 256, 0, L.stream>>>(L.N, x, L.x32);
   ck(cudaGetLastError(), "Forward Solve Error =");
   ck(cudaGraphLaunch(L.sweeps, L.stream), "Forward Solve Error =");
@@ -232,7 +323,8 @@ extern "C" void unload_external_lu_solver(void) {
   LegacyLU &L = g_lu;
   if (!L.loaded) return;
   cudaStreamSynchronize(L.stream);
-  cudaGraphExecDestroy(L.sweeps);
+  delete L.wave;  // its stream, sweeps and buffers
+  if (L.sweeps) cudaGraphExecDestroy(L.sweeps);
   cudaFree(L.dptr);
   cudaFree(L.dinv);
   cudaFree(L.x32);

@@ -679,13 +679,12 @@ __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__r
 // ILU(0) inner update: x += alpha p (FP64 x, FP32 p), r32 = r32 - alpha q
 // rounded once; the sweeps then read r32 directly.  Four unknowns per thread
 // (the padded vector length is a multiple of 16).
-__global__ void __launch_bounds__(NTHR) k_update_x32(Geo g, UpdateArgs a) {
+__device__ __forceinline__ void update_x32_body(const Geo &g, const UpdateArgs &a, long long t0, long long stride) {
   const volatile SolveState *vs = a.st;
   if (vs->status != ST_RUNNING) return;
   const double alpha = vs->alpha;
   const long long n4 = g.Np / 4;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = t0; t < n4; t += stride) {
     const long long id = 4 * t;
     double2 x0 = *reinterpret_cast<const double2 *>(a.x + id);
     double2 x1 = *reinterpret_cast<const double2 *>(a.x + id + 2);
@@ -704,6 +703,9 @@ __global__ void __launch_bounds__(NTHR) k_update_x32(Geo g, UpdateArgs a) {
     *reinterpret_cast<double2 *>(a.x + id + 2) = x1;
     *reinterpret_cast<float4 *>(a.r32 + id) = rv;
   }
+}
+__global__ void __launch_bounds__(NTHR) k_update_x32(Geo g, UpdateArgs a) {
+  update_x32_body(g, a, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
 // r = b - q (the FP64 true residual of a reliable update, q = A x) and its
@@ -1191,6 +1193,8 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   m.rh = upload_1based(mesh->rh, nr, this, &st);
   m.dt = upload_1based(mesh->dt, nt - 1, this, &st);
   m.dp = upload_1based(mesh->dp, np, this, &st);
+  m.th = upload_1based(mesh->th, nt, this, &st);
+  m.ph = upload_1based(mesh->ph, np, this, &st);
   if (st != POT3D_OK) return st;
   m.dr1 = mesh->dr[0];
   m.drn = mesh->dr[nr - 2];
@@ -1923,7 +1927,8 @@ __device__ __forceinline__ int batch_find(const BatchInst *__restrict__ in, int 
   return i;
 }
 
-// MODE_PCG (diagonal preconditioner) or MODE_PCGZ (z from the ILU(0) sweeps).
+// MODE_PCG (diagonal preconditioner) or MODE_PCGZ (z from the ILU(0) sweeps),
+// and their FP32-inner forms MODE_PCG32 / MODE_PCGZ32.
 template <int MODE>
 __global__ void __launch_bounds__(NTHR, 2) k_stencil_batch(const BatchInst *__restrict__ in, int n, int par) {
   const int i = batch_find(in, n, blockIdx.x, BATCH_STENCIL);
@@ -1933,21 +1938,24 @@ __global__ void __launch_bounds__(NTHR, 2) k_stencil_batch(const BatchInst *__re
   const StencilArgs a = I.sa[par];
   const unsigned local = blockIdx.x - I.off_s;
   if (threadIdx.x == 0) {  // the thread that issues the TMA loads
-    tma_acquire_desc(&I.maps[par].m64[0]);
+    if (MODE == MODE_PCG || MODE == MODE_PCGZ) tma_acquire_desc(&I.maps[par].m64[0]);
     if (MODE == MODE_PCG) tma_acquire_desc(&I.maps[par].m64[1]);
     tma_acquire_desc(&I.maps[par].m32[0]);
+    if (MODE == MODE_PCG32 || MODE == MODE_PCGZ32) tma_acquire_desc(&I.maps[par].m32[1]);
+    if (MODE == MODE_PCG32) tma_acquire_desc(&I.maps[par].m32[2]);
   }
   stencil_body<MODE>(I.maps[par], g, m, a, local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
 }
 
-// UPD_ITER with the diagonal preconditioner, UPD_ZDOT after the ILU(0) sweeps.
-template <int KIND, bool ZIN>
+// UPD_ITER with the diagonal preconditioner, UPD_ZDOT after the ILU(0) sweeps
+// (R32: the FP32-inner forms).
+template <int KIND, bool ZIN, bool R32 = false>
 __global__ void __launch_bounds__(NTHR) k_update_batch(const BatchInst *__restrict__ in, int n, int par) {
   const int i = batch_find(in, n, blockIdx.x, BATCH_UPDATE);
   const BatchInst &I = in[i];
   const Geo &g = I.g;
   const unsigned local = blockIdx.x - I.off_u;
-  update_body<KIND, ZIN>(g, I.m, I.ua[par], local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
+  update_body<KIND, ZIN, R32>(g, I.m, I.ua[par], local % g.nit, (local / g.nit) % g.njt, local / (g.nit * g.njt));
 }
 
 __global__ void __launch_bounds__(NTHR) k_update_r32_batch(const BatchInst *__restrict__ in, int n, int par) {
@@ -1955,6 +1963,13 @@ __global__ void __launch_bounds__(NTHR) k_update_r32_batch(const BatchInst *__re
   const BatchInst &I = in[i];
   const unsigned local = blockIdx.x - I.off_r;
   update_r32_body(I.g, I.ua[par], (long long)local * NTHR + threadIdx.x, (long long)I.nb_r * NTHR);
+}
+// FP32-inner ILU(0): x += alpha p (FP64 x), r32 -= alpha q, every running case.
+__global__ void __launch_bounds__(NTHR) k_update_x32_batch(const BatchInst *__restrict__ in, int n, int par) {
+  const int i = batch_find(in, n, blockIdx.x, BATCH_R32);
+  const BatchInst &I = in[i];
+  const unsigned local = blockIdx.x - I.off_r;
+  update_x32_body(I.g, I.ua[par], (long long)local * NTHR + threadIdx.x, (long long)I.nb_r * NTHR);
 }
 
 struct Batch {
@@ -1971,13 +1986,22 @@ struct Batch {
   int U = 8;
   int tk = 0;      // stencil planes per block (0 = per-case default)
   int ifprec = 1;  // 1: diagonal preconditioner; 2: ILU(0) with batched wavefront sweeps
+  int precision = POT3D_FP64;  // or POT3D_FP32_REFINED: FP32-inner iterations, per-case reliable updates
   DiluBatch *wave = nullptr;
   unsigned nblk_r = 0;
+  std::vector<double *> guess;  // per case: initial guess (padded, device) or null for zero
+  // refined mode, per case: r.z at the last FP64 residual and its iteration,
+  // iterations at the start of the last graph, updates made, stagnant updates
+  // in a row, and the iterations done before a switch to FP64 PCG
+  std::vector<double> rho_ref;
+  std::vector<int> ncg_ref, ncg0, n_ref, stagnant, ncg_before_fp64;
   ~Batch() {
     if (graph) cudaGraphExecDestroy(graph);
     dilu_batch_destroy(wave);
     for (Solver *s : inst)  // the cases run on the batch's stream, destroyed below
       if (s && s->stream == stream) s->stream = nullptr;
+    for (double *g : guess)
+      if (g) cudaFree(g);
     if (d_tab) cudaFree(d_tab);
     if (pin) cudaFreeHost(pin);
     if (ev0) cudaEventDestroy(ev0);
@@ -2036,6 +2060,25 @@ static int batch_table(Batch &B) {
       ua.st = s.d_state;
       ua.partials = s.d_partials;
       int st;
+      if (B.precision == POT3D_FP32_REFINED) {  // the operands of launch_iteration32
+        float *o32 = par == 0 ? s.m_p32a : s.m_p32b, *n32 = par == 0 ? s.m_p32b : s.m_p32a;
+        sa.p_new32 = n32;
+        sa.q32 = s.m_q32;
+        ua.p32 = n32;
+        ua.q32 = s.m_q32;
+        ua.r32 = s.r32_inner();
+        ua.z32 = ilu ? dilu_z32(&s) : nullptr;
+        StencilMaps &mp = I.maps[par];
+        if ((st = s.tensor_map(o32, false, &mp.m32[0]))) return st;
+        if (ilu) {
+          if ((st = s.tensor_map(dilu_z32(&s), false, &mp.m32[1]))) return st;
+          mp.m32[2] = mp.m32[0];
+        } else if ((st = s.tensor_map(s.m_r32, false, &mp.m32[1])) || (st = s.tensor_map(s.d_ai, false, &mp.m32[2]))) {
+          return st;
+        }
+        mp.m64[0] = mp.m64[1] = mp.m32[0];
+        continue;
+      }
       if (ilu) {  // the operands of launch_iteration's ifprec=2 branch
         sa.z32 = dilu_z32(&s);
         ua.z32 = dilu_z32(&s);
@@ -2070,14 +2113,25 @@ static int batch_table(Batch &B) {
 }
 
 static int batch_init(Batch &B, int ncgmax, double epscg) {
-  for (Solver *sp : B.inst) {
-    Solver &s = *sp;
+  const size_t nc = B.inst.size();
+  B.rho_ref.assign(nc, 0.0);
+  B.ncg_ref.assign(nc, 0);
+  B.ncg0.assign(nc, 0);
+  B.n_ref.assign(nc, 0);
+  B.stagnant.assign(nc, 0);
+  B.ncg_before_fp64.assign(nc, -1);
+  for (size_t q = 0; q < nc; q++) {
+    Solver &s = *B.inst[q];
+    const bool guessed = q < B.guess.size() && B.guess[q];
     SolveState s0{};
     s0.epscg = epscg;
     s0.ncgmax = ncgmax;
     s0.hist = nullptr;
     CK(cudaMemcpyAsync(s.d_state, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, B.stream));
-    CK(cudaMemsetAsync(s.d_x, 0, sizeof(double) * s.g.Np, B.stream));
+    if (guessed)
+      CK(cudaMemcpyAsync(s.d_x, B.guess[q], sizeof(double) * s.g.Np, cudaMemcpyDeviceToDevice, B.stream));
+    else
+      CK(cudaMemsetAsync(s.d_x, 0, sizeof(double) * s.g.Np, B.stream));
     CK(cudaMemsetAsync(s.d_p, 0, sizeof(double) * s.g.Np, B.stream));
     CK(cudaMemsetAsync(s.d_s1p, 0, sizeof(double) * 2 * s.g.NRP, B.stream));
     CK(cudaMemcpyAsync(s.d_r, s.d_b, sizeof(double) * s.g.Np, cudaMemcpyDeviceToDevice, B.stream));
@@ -2091,20 +2145,51 @@ static int batch_init(Batch &B, int ncgmax, double epscg) {
     ua.s1z_part = s.d_s1z;
     ua.st = s.d_state;
     ua.partials = s.d_partials;
+    int st;
+    if (B.precision == POT3D_FP32_REFINED) {
+      // mixed_solve's prologue: bdotb, the FP64 initial residual of the
+      // guess and its r.z, with the case's own (unbatched) kernels
+      CK(cudaMemsetAsync(s.m_p32a, 0, sizeof(float) * s.g.Np, B.stream));
+      k_cast_r32<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_r, s.r32_inner());
+      if (B.ifprec == 2) {
+        if ((st = dilu_reset(&s)) || (st = dilu_sweeps(&s, false))) return st;
+        ua.z32 = dilu_z32(&s);
+        k_update<UPD_BDOTB, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      } else {
+        k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      }
+      if (guessed) {
+        if ((st = s.ax_padded(s.d_x, s.d_q))) return st;
+        k_resid_cast<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_b, s.d_q, s.d_r, s.r32_inner());
+        if (B.ifprec == 2 && (st = dilu_sweeps(&s, false))) return st;
+      }
+      if (B.ifprec == 2)
+        k_update<UPD_INIT, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      else
+        k_update<UPD_INIT, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      continue;
+    }
     if (B.ifprec == 2) {
       // bdotb = b . M^-1 b and the initial z, rho as cgsolve_padded does,
       // with the case's own (unbatched) sweeps
-      int st;
       if ((st = dilu_reset(&s))) return st;
       ua.z32 = dilu_z32(&s);
       k_cast_r32<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_r, dilu_r32(&s));
       if ((st = dilu_sweeps(&s, false))) return st;
       k_update<UPD_BDOTB, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      if (guessed) {
+        if ((st = s.ax_padded(s.d_x, s.d_q))) return st;
+        k_axpy_sub<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_q, s.d_r);
+      }
       k_cast_r32<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_r, dilu_r32(&s));
       if ((st = dilu_sweeps(&s, false))) return st;
       k_update<UPD_INIT, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
     } else {
       k_update<UPD_BDOTB, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
+      if (guessed) {
+        if ((st = s.ax_padded(s.d_x, s.d_q))) return st;
+        k_axpy_sub<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_q, s.d_r);
+      }
       k_update<UPD_INIT, false><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
     }
   }
@@ -2117,6 +2202,18 @@ static int batch_init(Batch &B, int ncgmax, double epscg) {
 
 static void batch_iteration(Batch &B, int par) {
   const int n = (int)B.act.size();
+  if (B.precision == POT3D_FP32_REFINED) {  // launch_iteration32's sequence, every running case per launch
+    if (B.ifprec == 2) {
+      k_stencil_batch<MODE_PCGZ32><<<B.nblk_s, NTHR, StageLayout<MODE_PCGZ32>::smem, B.stream>>>(B.d_tab, n, par);
+      k_update_x32_batch<<<B.nblk_r, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+      dilu_batch_sweeps(B.wave, B.stream);
+      k_update_batch<UPD_ZDOT, true, true><<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+    } else {
+      k_stencil_batch<MODE_PCG32><<<B.nblk_s, NTHR, StageLayout<MODE_PCG32>::smem, B.stream>>>(B.d_tab, n, par);
+      k_update_batch<UPD_ITER, false, true><<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+    }
+    return;
+  }
   if (B.ifprec == 2) {  // launch_iteration's ifprec=2 sequence, every running case per launch
     k_stencil_batch<MODE_PCGZ><<<B.nblk_s, NTHR, StageLayout<MODE_PCGZ>::smem, B.stream>>>(B.d_tab, n, par);
     k_update_r32_batch<<<B.nblk_r, NTHR, 0, B.stream>>>(B.d_tab, n, par);
@@ -2171,9 +2268,14 @@ struct pot3d_gpu_batch {
   pot3d::Batch b;
 };
 
-extern "C" int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
-                                         const double *pm_r1s, int tk, int ifprec, pot3d_gpu_batch **out) {
+extern "C" int pot3d_gpu_batch_create_mode(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                                           const double *pm_r1s, int tk, int ifprec, int precision,
+                                           pot3d_gpu_batch **out) {
   using namespace pot3d;
+  if (precision != POT3D_FP64 && precision != POT3D_FP32_REFINED) {
+    pot3d_set_error("pot3d_gpu_batch_create: precision must be POT3D_FP64 or POT3D_FP32_REFINED");
+    return POT3D_ERR_ARG;
+  }
   if (n < 1 || !meshes || !br0s || !pm_r1s || !out) {
     pot3d_set_error("pot3d_gpu_batch_create: invalid arguments");
     return POT3D_ERR_ARG;
@@ -2190,6 +2292,8 @@ extern "C" int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, cons
   pot3d_gpu_batch *h = new pot3d_gpu_batch();
   Batch &B = h->b;
   B.ifprec = ifprec;
+  B.precision = precision;
+  B.guess.assign(n, nullptr);
   int st = pot3d_cuda_status(cudaStreamCreate(&B.stream), "cudaStreamCreate");
   if (!st) st = pot3d_cuda_status(cudaEventCreate(&B.ev0), "cudaEventCreate");
   if (!st) st = pot3d_cuda_status(cudaEventCreate(&B.ev1), "cudaEventCreate");
@@ -2198,7 +2302,7 @@ extern "C" int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, cons
   for (int q = 0; q < n && !st; q++) {
     Solver *s = new Solver();
     B.inst.push_back(s);
-    st = s->setup(&meshes[q], br0s[q], nullptr, pm_r1s[q], ifprec, POT3D_FP64);
+    st = s->setup(&meshes[q], br0s[q], nullptr, pm_r1s[q], ifprec, precision);
     if (!st) {
       s->tk_default = s->g.tk;
       s->nkc_default = s->g.nkc;
@@ -2224,6 +2328,13 @@ extern "C" int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, cons
                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 StageLayout<MODE_PCGZ>::smem),
                            "cudaFuncSetAttribute(k_stencil_batch)");
+  for (int m : {MODE_PCG32, MODE_PCGZ32}) {
+    if (st) break;
+    const void *fn = m == MODE_PCG32 ? (const void *)k_stencil_batch<MODE_PCG32> : (const void *)k_stencil_batch<MODE_PCGZ32>;
+    const int smem = m == MODE_PCG32 ? StageLayout<MODE_PCG32>::smem : StageLayout<MODE_PCGZ32>::smem;
+    st = pot3d_cuda_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                           "cudaFuncSetAttribute(k_stencil_batch)");
+  }
   if (!st && ifprec == 2) st = dilu_batch_setup(B.inst.data(), n, B.stream, &B.wave);
   if (st) {
     delete h;
@@ -2234,9 +2345,35 @@ extern "C" int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, cons
   return POT3D_OK;
 }
 
+extern "C" int pot3d_gpu_batch_create_ex(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
+                                         const double *pm_r1s, int tk, int ifprec, pot3d_gpu_batch **out) {
+  return pot3d_gpu_batch_create_mode(n, meshes, br0s, pm_r1s, tk, ifprec, POT3D_FP64, out);
+}
+
 extern "C" int pot3d_gpu_batch_create(int n, const pot3d_mesh_t *meshes, const double *const *br0s,
                                       const double *pm_r1s, int tk, pot3d_gpu_batch **out) {
-  return pot3d_gpu_batch_create_ex(n, meshes, br0s, pm_r1s, tk, 1, out);
+  return pot3d_gpu_batch_create_mode(n, meshes, br0s, pm_r1s, tk, 1, POT3D_FP64, out);
+}
+
+extern "C" int pot3d_gpu_batch_set_guess(pot3d_gpu_batch *h, int i, const double *x) {
+  using namespace pot3d;
+  if (!h || i < 0 || i >= (int)h->b.inst.size()) {
+    pot3d_set_error("pot3d_gpu_batch_set_guess: invalid arguments");
+    return POT3D_ERR_ARG;
+  }
+  Batch &B = h->b;
+  Solver &s = *B.inst[i];
+  if (!x) {  // back to a zero guess
+    if (B.guess[i]) cudaFree(B.guess[i]);
+    B.guess[i] = nullptr;
+    return POT3D_OK;
+  }
+  if (!B.guess[i]) CK(cudaMalloc(&B.guess[i], sizeof(double) * s.g.Np));
+  int st;
+  CK(cudaMemcpyAsync(s.d_tmp, x, sizeof(double) * s.g.N, cudaMemcpyHostToDevice, B.stream));
+  if ((st = s.pack(s.d_tmp, B.guess[i]))) return st;
+  CK(cudaStreamSynchronize(B.stream));
+  return POT3D_OK;
 }
 
 // Autotuner: times `iters` batched iterations of all cases for each candidate
@@ -2304,7 +2441,50 @@ extern "C" int pot3d_gpu_batch_solve(pot3d_gpu_batch *h, int ncgmax, double epsc
   // only running cases' tiles) and re-capture when the set changed.
   long long last_total = -1;
   int stalls = 0;
+  const bool refined = B.precision == POT3D_FP32_REFINED;
+  for (int q = 0; q < n; q++) B.rho_ref[q] = B.pin[q].rho;
+  bool after_graph = false;
   for (;;) {
+    if (refined && after_graph) {
+      // Reliable updates of the cases that need one (mixed_solve's rules,
+      // per case), made with each case's own kernels, then one poll.
+      std::vector<int> ru;
+      for (int q : B.act) {
+        const SolveState &S = B.pin[q];
+        if (S.status != ST_RUNNING && S.status != ST_CONVERGED && S.status != ST_MAXIT) continue;
+        if (B.ncg_before_fp64[q] >= 0) continue;  // finished by FP64 PCG
+        if (S.status == ST_CONVERGED || S.status == ST_MAXIT || S.rho < B.inst[q]->refine_ratio * B.rho_ref[q] ||
+            S.rho > 100.0 * B.rho_ref[q] || S.ncg - B.ncg_ref[q] >= 1000)
+          ru.push_back(q);
+      }
+      if (!ru.empty()) {
+        for (int q : ru)
+          if ((st = B.inst[q]->reliable_update())) return st;
+        std::vector<int> ran(n, 0);
+        for (int q : ru) ran[q] = B.pin[q].ncg - B.ncg0[q];
+        if ((st = batch_poll(B))) return st;
+        for (int q : ru) {
+          Solver &s = *B.inst[q];
+          const SolveState &S = B.pin[q];
+          B.n_ref[q]++;
+          if (S.status != ST_RUNNING) continue;
+          if (ran[q] & 1)  // stopped after an odd number of iterations: newest p in the other buffer
+            CK(cudaMemcpyAsync(s.m_p32a, s.m_p32b, sizeof(float) * s.g.Np, cudaMemcpyDeviceToDevice, B.stream));
+          if (S.ncg - B.ncg_ref[q] >= 10) B.stagnant[q] = S.rho > s.stall_drop * B.rho_ref[q] ? B.stagnant[q] + 1 : 0;
+          B.rho_ref[q] = S.rho;
+          B.ncg_ref[q] = S.ncg;
+          if (B.stagnant[q] >= s.stall_limit) {
+            // this case's FP32 recurrence stopped tracking its FP64 residual:
+            // FP64 PCG (same preconditioner) from its current x, on its own
+            B.ncg_before_fp64[q] = S.ncg;
+            int ie = 1;
+            pot3d_solve_info_t inf2{};
+            if ((st = s.cgsolve_padded(false, std::max(1, ncgmax - S.ncg), epscg, &ie, &inf2))) return st;
+          }
+        }
+        if ((st = batch_poll(B))) return st;
+      }
+    }
     std::vector<int> run;
     long long total = 0;  // iterations of all cases, finished ones included
     for (int q : B.act)
@@ -2324,9 +2504,11 @@ extern "C" int pot3d_gpu_batch_solve(pot3d_gpu_batch *h, int ncgmax, double epsc
       B.act = run;
       if ((st = batch_table(B)) || (st = batch_capture(B))) return st;
     }
+    for (int q : run) B.ncg0[q] = B.pin[q].ncg;
     CK(cudaGraphLaunch(B.graph, B.stream));
     launches += 2LL * B.U * batch_launches_per_iteration(B);
     if ((st = batch_poll(B))) return st;
+    after_graph = true;
   }
   CK(cudaEventRecord(B.ev1, B.stream));
   CK(cudaEventSynchronize(B.ev1));
@@ -2336,7 +2518,8 @@ extern "C" int pot3d_gpu_batch_solve(pot3d_gpu_batch *h, int ncgmax, double epsc
     if (ierr) ierr[q] = B.pin[q].status == ST_CONVERGED ? 0 : 1;
     if (info) {
       info[q] = pot3d_solve_info_t{};
-      info[q].ncg = B.pin[q].ncg;
+      info[q].ncg = B.pin[q].ncg + std::max(0, B.ncg_before_fp64[q]);
+      info[q].n_refine = refined ? B.n_ref[q] : 0;
       info[q].epsn = B.pin[q].epsn;
       info[q].seconds = ms * 1e-3;
       info[q].kernel_launches = launches;

@@ -28,6 +28,7 @@ constexpr int SROW = TI + 4;  // shared-memory row: [pad, halo-, 64 own, halo+, 
 struct DevMesh {
   const double *drh, *dth, *sth_i, *dp_i, *dph, *st, *dt_i, *sth, *r2, *dr_i;
   const double *dr, *rh, *dt, *dp;
+  const double *th, *ph;    // half-mesh coordinates (readbr's interpolation points)
   const double *br0, *br1;  // (nt,np) column-major, 0-based
   double dr1, drn, pm_r1, pl_i;
 };

@@ -102,6 +102,8 @@ int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, 
 int dilu_reset(Solver *s);
 int dilu_status(Solver *s);  // POT3D_ERR_TIMEOUT if a sweep gave up waiting
 int dilu_test_stall(Solver *s, unsigned spin_limit);  // a sweep whose waits must run out
+// Sweeps for a factored 1-based CSR with the 7-point pattern of s->g's grid.
+int dilu_setup_csr(Solver *s, const int *ia, const int *ja, const int *dptr, const float *a, const float *dinv);
 int dilu_time(Solver *s, int reps, double ms[2]);
 int dilu_diag(Solver *s, float *d_host, float *dinv_host);
 int dilu_sweep_launches(Solver *s);

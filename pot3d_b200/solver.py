@@ -66,6 +66,22 @@ class Pot3dSolver:
         self._br0 = b
         check(_lib.lib().pot3d_gpu_set_br0(self._h, dptr(b)))
 
+    def br0_from_map(self, tn, pn, fi, option=None, do_not_balance_flux=False) -> np.ndarray:
+        """readbr on the device: interpolate the map fi[ntn, npn] (Fortran
+        axis order, scales tn, pn) onto the mesh, pole rows, flux balance and
+        'open' |Br|; the result becomes this solve's br0 and is returned
+        (nt, np) in Fortran order."""
+        from .host import OPTION_CODE
+        opt = self.option if option is None else option
+        fi = np.asfortranarray(np.asarray(fi, dtype=np.float64))
+        tn = np.ascontiguousarray(tn, dtype=np.float64)
+        pn = np.ascontiguousarray(pn, dtype=np.float64)
+        out = np.zeros((self.mesh.nt, self.mesh.np), order="F")
+        check(_lib.lib().pot3d_gpu_br0_from_map(self._h, fi.shape[0], fi.shape[1], dptr(tn), dptr(pn), dptr(fi),
+                                                OPTION_CODE[opt], int(do_not_balance_flux), dptr(out)))
+        self._br0 = out
+        return out
+
     def rhs(self) -> np.ndarray:
         b = np.zeros(self.N)
         check(_lib.lib().pot3d_gpu_rhs(self._h, dptr(b)))
@@ -212,10 +228,11 @@ class BatchSolver:
     all unfinished cases, each case stops at its own ernorm criterion.  FP64
     PCG with the diagonal preconditioner (ifprec=1) or ILU(0) (ifprec=2: both
     triangular sweeps of all cases run in one wavefront kernel per
-    direction), zero initial guess.
+    direction), FP64 or FP32-inner / FP64-refined (precision), from zero or
+    from per-case guesses (set_guess).
     """
 
-    def __init__(self, meshes, br0s, pm_r1s, tk: int = 0, ifprec: int = 1):
+    def __init__(self, meshes, br0s, pm_r1s, tk: int = 0, ifprec: int = 1, precision: str = "fp64"):
         if not (len(meshes) == len(br0s) == len(pm_r1s)) or not meshes:
             raise ValueError("meshes, br0s and pm_r1s must be non-empty and of equal length")
         n = len(meshes)
@@ -229,7 +246,8 @@ class BatchSolver:
         self._brp = (C.POINTER(C.c_double) * n)(*[dptr(b) for b in self._br])
         self._r1 = np.ascontiguousarray(pm_r1s, dtype=np.float64)
         h = C.c_void_p()
-        check(_lib.lib().pot3d_gpu_batch_create_ex(n, self._mcs, self._brp, dptr(self._r1), tk, ifprec, C.byref(h)))
+        check(_lib.lib().pot3d_gpu_batch_create_mode(n, self._mcs, self._brp, dptr(self._r1), tk, ifprec,
+                                                     PRECISION[precision], C.byref(h)))
         self._h = h
         self.n = n
         self.tk = tk
@@ -273,6 +291,18 @@ class BatchSolver:
         self.infos = list(infos)
         self.seconds = sec.value
         return list(ierr)
+
+    def set_guess(self, i: int, x=None):
+        """Initial guess of case i (packed layout, length N_i) for later
+        solves; None returns to a zero guess."""
+        if x is None:
+            check(_lib.lib().pot3d_gpu_batch_set_guess(self._h, i, None))
+            return
+        m = self.meshes[i]
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != (m.nr - 2) * (m.nt - 2) * (m.np - 2):
+            raise ValueError("guess has the wrong length for its case")
+        check(_lib.lib().pot3d_gpu_batch_set_guess(self._h, i, dptr(x)))
 
     def solution(self, i: int) -> np.ndarray:
         """Interior solution of case i, packed layout (length N_i)."""

@@ -1,16 +1,20 @@
-"""Learned warm start: training pairs from the plain solver, training, and the
-held-out evaluation of PCG from the predicted guess against PCG from zero.
+"""Learned warm start: training pairs from the solver, training, and the
+held-out evaluation of the solve from the predicted guess against the solve
+from zero.
 
     python -m pot3d_b200.warmstart --nr 127 --nt 181 --np 361 \\
-        --train 2000 --test 200 --epochs 20 --out results.json [--save model.npz]
-        [--ifprec 2] [--no-refined]
+        --train 2000 --test 200 --epochs 20 --out record.json [--save model.npz]
+        [--ifprec 2] [--precision fp32_refined] [--plain]
 
 Training pairs are (Br0 map, phi) of seeded synthetic PFSS cases solved by
-the FP64 GPU PCG (`--train-eps`, default 1e-7: the network is far less
-accurate than that).  The evaluation solves every held-out case to the
-unchanged tolerance (epscg 1e-9) from x = 0 and from the network's guess;
-PCG decides convergence either way, so a poor guess costs iterations,
-never accuracy.
+the GPU solver (ILU(0), FP32-refined by default) to `--train-eps` (default
+1e-9).  The evaluation solves every held-out case to the unchanged
+tolerance (epscg 1e-9) from x = 0 and from the network's guess with the same
+solver (and, with --plain, the plain FP64 diagonal PCG from zero); PCG
+decides convergence either way, so a poor guess costs iterations, never
+accuracy.  Each row records both iteration counts and times (inference
+included) and how far the guessed solve's solution lies from the one from
+zero.
 """
 from __future__ import annotations
 
@@ -156,9 +160,9 @@ def train(model: FNO, inputs: Inputs, br0n, tgt, epochs, batch, lr, seed=0, log=
     return hist
 
 
-def evaluate(model: FNO, inputs: Inputs, mesh, solver, seeds, lmax, nbip, eps=1e-9, solver32=None):
-    """Per held-out case: PCG to eps from zero and from the predicted guess
-    (and, with solver32, the FP32-refined solve from zero and from the guess)."""
+def evaluate(model: FNO, inputs: Inputs, mesh, solver, seeds, lmax, nbip, eps=1e-9, plain=None):
+    """Per held-out case: the solver to eps from zero and from the predicted
+    guess (and, with `plain`, that solver from zero as the baseline)."""
     import torch
     N = solver.N
     rows = []
@@ -172,7 +176,8 @@ def evaluate(model: FNO, inputs: Inputs, mesh, solver, seeds, lmax, nbip, eps=1e
         x.zero_()
         r.copy_(b)
         torch.cuda.synchronize()
-        solver.cgsolve_dev(x, r, epscg=eps)
+        if solver.cgsolve_dev(x, r, epscg=eps) != 0:
+            raise RuntimeError(f"held-out solve {sd} from zero did not converge")
         z = solver.last_info
         xs = x.clone()
         v, s = inputs.normalized(br0)
@@ -186,41 +191,38 @@ def evaluate(model: FNO, inputs: Inputs, mesh, solver, seeds, lmax, nbip, eps=1e
         x.copy_(guess)
         r.copy_(b)
         torch.cuda.synchronize()
-        solver.cgsolve_dev(x, r, epscg=eps)
+        if solver.cgsolve_dev(x, r, epscg=eps) != 0:
+            raise RuntimeError(f"held-out solve {sd} from the guess did not converge")
         w = solver.last_info
         row = dict(seed=int(sd), ncg_zero=z.ncg, s_zero=z.seconds, ncg_guess=w.ncg, s_guess=w.seconds,
-                   s_inference=t_inf, guess_rel_err=err, epsn_guess=w.epsn)
-        if solver32 is not None:
-            _set_br0(solver32, br0)
-            for tag, start in (("r32_zero", None), ("r32_guess", guess)):
-                if start is None:
-                    x.zero_()
-                else:
-                    x.copy_(start)
-                r.copy_(b)
-                torch.cuda.synchronize()
-                solver32.cgsolve_dev(x, r, epscg=eps)
-                q = solver32.last_info
-                row[f"ncg_{tag}"] = q.ncg
-                row[f"s_{tag}"] = q.seconds
-                row[f"refine_{tag}"] = q.n_refine
-                row[f"err_{tag}"] = float(torch.linalg.norm(x - xs) / torch.linalg.norm(xs))
+                   s_inference=t_inf, guess_rel_err=err, epsn_guess=w.epsn,
+                   sol_rel_diff=float(torch.linalg.norm(x - xs) / torch.linalg.norm(xs)))
+        if plain is not None:
+            _set_br0(plain, br0)
+            x.zero_()
+            r.copy_(b)
+            torch.cuda.synchronize()
+            if plain.cgsolve_dev(x, r, epscg=eps) != 0:
+                raise RuntimeError(f"plain solve {sd} did not converge")
+            row["ncg_plain"] = plain.last_info.ncg
+            row["s_plain"] = plain.last_info.seconds
         rows.append(row)
     a = lambda k: np.array([q[k] for q in rows])
     summ = dict(cases=len(rows), ncg_zero_mean=float(a("ncg_zero").mean()), ncg_guess_mean=float(a("ncg_guess").mean()),
                 ncg_zero_median=float(np.median(a("ncg_zero"))), ncg_guess_median=float(np.median(a("ncg_guess"))),
                 s_zero_mean=float(a("s_zero").mean()),
                 s_guess_mean=float((a("s_guess") + a("s_inference")).mean()),
+                s_inference_mean=float(a("s_inference").mean()),
                 guess_rel_err_mean=float(a("guess_rel_err").mean()),
-                iteration_ratio=float(a("ncg_guess").mean() / a("ncg_zero").mean()))
-    if solver32 is not None:
-        for tag in ("r32_zero", "r32_guess"):
-            summ[f"ncg_{tag}_mean"] = float(a(f"ncg_{tag}").mean())
-            summ[f"s_{tag}_mean"] = float(a(f"s_{tag}").mean()) + (
-                float(a("s_inference").mean()) if tag == "r32_guess" else 0.0)
-            summ[f"sol_err_{tag}_max"] = float(a(f"err_{tag}").max())
-        summ["speedup_learned_refined_vs_plain"] = summ["s_zero_mean"] / summ["s_r32_guess_mean"]
-        summ["speedup_learned_plain_vs_plain"] = summ["s_zero_mean"] / summ["s_guess_mean"]
+                guess_rel_err_max=float(a("guess_rel_err").max()),
+                sol_rel_diff_max=float(a("sol_rel_diff").max()),
+                iteration_ratio=float(a("ncg_guess").mean() / a("ncg_zero").mean()),
+                time_ratio=float((a("s_guess") + a("s_inference")).mean() / a("s_zero").mean()),
+                fewer_iterations_cases=int((a("ncg_guess") < a("ncg_zero")).sum()))
+    if plain is not None:
+        summ["ncg_plain_mean"] = float(a("ncg_plain").mean())
+        summ["s_plain_mean"] = float(a("s_plain").mean())
+        summ["speedup_learned_vs_plain"] = summ["s_plain_mean"] / summ["s_guess_mean"]
     return summ, rows
 
 
@@ -235,19 +237,21 @@ def main(argv=None):
     ap.add_argument("--test", type=int, default=200)
     ap.add_argument("--train-seed0", type=int, default=1000)
     ap.add_argument("--test-seed0", type=int, default=5000)
-    ap.add_argument("--train-eps", type=float, default=1e-7)
+    ap.add_argument("--train-eps", type=float, default=1e-9)
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default="warmstart.json")
     ap.add_argument("--save", default="")
     ap.add_argument("--no-augment", action="store_true")
-    ap.add_argument("--ifprec", type=int, default=1, help="preconditioner of the generating and evaluating solves")
-    ap.add_argument("--no-refined", action="store_true", help="skip the FP32-refined evaluation solves")
+    ap.add_argument("--ifprec", type=int, default=2, help="preconditioner of the generating and evaluating solves")
+    ap.add_argument("--precision", default="fp32_refined", choices=["fp64", "fp32_refined"])
+    ap.add_argument("--plain", action="store_true", help="also time the plain FP64 diagonal PCG from zero")
     args = ap.parse_args(argv)
     import torch
     mesh = host.make_mesh(args.nr, args.nt, args.np)
-    solver = Pot3dSolver(mesh, case_br0(mesh, args.train_seed0, args.lmax, args.nbip), ifprec=args.ifprec)
+    solver = Pot3dSolver(mesh, case_br0(mesh, args.train_seed0, args.lmax, args.nbip), ifprec=args.ifprec,
+                         precision=args.precision)
     model = FNO(grid_from_mesh(mesh))
     inputs = Inputs(model)
     t0 = time.time()
@@ -264,10 +268,9 @@ def main(argv=None):
     from .tc import check_errors
     check_errors()
     del br0n, tgt
-    solver32 = None if args.no_refined else Pot3dSolver(mesh, case_br0(mesh, args.test_seed0, args.lmax, args.nbip),
-                                                        precision="fp32_refined")
+    plain = Pot3dSolver(mesh, case_br0(mesh, args.test_seed0, args.lmax, args.nbip), ifprec=1) if args.plain else None
     summ, rows = evaluate(model, inputs, mesh, solver, range(args.test_seed0, args.test_seed0 + args.test),
-                          args.lmax, args.nbip, solver32=solver32)
+                          args.lmax, args.nbip, plain=plain)
     t3 = time.time()
     rep = dict(config=vars(args), generation=dict(seconds=t1 - t0, **gstat), training=dict(seconds=t2 - t1,
                loss_history=hist), evaluation=dict(seconds=t3 - t2, **summ), cases=rows)

@@ -111,3 +111,70 @@ def test_batch_rejects_bad_preconditioner(cuda):
     mesh, br0 = _cases()[0]
     with pytest.raises(Pot3dError):
         BatchSolver([mesh], [br0], [1.0], ifprec=3)
+
+
+@pytest.mark.parametrize("ifprec", [1, 2])
+def test_batch_matches_the_oracle(cuda, ifprec):
+    """Every case of an uneven batch (own grid, map and source-surface
+    radius) solved to 1e-11 by the batched kernels lands on the oracle's
+    solution of that case (the reference's CPU PCG with the same
+    preconditioner): relative L2 <= 1e-8 on the packed solution."""
+    import oracle as O
+    cases = _cases()
+    with BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * len(cases), ifprec=ifprec) as b:
+        assert b.solve(epscg=1e-11) == [0] * len(cases)
+        for q, (mesh, br0) in enumerate(cases):
+            mo = O.Mesh(mesh.nr, mesh.nt, mesh.np, *[getattr(mesh, f) for f in O.MESH_FIELDS])
+            o = O.Solver(mo, br0, "ss", ifprec)
+            ref = o.cgsolve(np.zeros(o.N), o.rhs(), epscg=1e-11)
+            x = b.solution(q)
+            assert np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"]), q
+            assert abs(b.infos[q].ncg - ref["ncg"]) <= max(2, ref["ncg"] // 50), (q, b.infos[q].ncg, ref["ncg"])
+
+
+@pytest.mark.parametrize("ifprec", [1, 2])
+def test_refined_batch_matches_the_oracle(cuda, ifprec):
+    """FP32-inner / FP64-refined batch (per-case reliable updates and
+    convergence on each case's FP64 residual): every case lands on the
+    oracle's FP64 solution at 1e-11, with iteration counts close to the
+    FP64 ones."""
+    import oracle as O
+    cases = _cases()
+    with BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * len(cases), ifprec=ifprec,
+                     precision="fp32_refined") as b:
+        assert b.solve(epscg=1e-11, ncgmax=20000) == [0] * len(cases)
+        for q, (mesh, br0) in enumerate(cases):
+            mo = O.Mesh(mesh.nr, mesh.nt, mesh.np, *[getattr(mesh, f) for f in O.MESH_FIELDS])
+            o = O.Solver(mo, br0, "ss", ifprec)
+            ref = o.cgsolve(np.zeros(o.N), o.rhs(), epscg=1e-11)
+            x = b.solution(q)
+            assert np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"]), q
+            assert b.infos[q].n_refine >= 1
+            assert b.infos[q].ncg <= 1.2 * ref["ncg"] + 16, (q, b.infos[q].ncg, ref["ncg"])
+        # from per-case guesses near the solutions: fewer iterations, same solutions
+        sols = [b.solution(q) for q in range(len(cases))]
+        ncg0 = [i.ncg for i in b.infos]
+        rng = np.random.default_rng(5)
+        for q, x in enumerate(sols):
+            b.set_guess(q, x * (1.0 + 1e-2 * rng.standard_normal(x.size)))
+        assert b.solve(epscg=1e-11, ncgmax=20000) == [0] * len(cases)
+        for q, x in enumerate(sols):
+            assert np.linalg.norm(b.solution(q) - x) <= 1e-8 * np.linalg.norm(x)
+            assert b.infos[q].ncg < ncg0[q]
+
+
+def test_batch_guess_fp64_and_reset(cuda):
+    cases = _cases()
+    with BatchSolver([c[0] for c in cases], [c[1] for c in cases], [PM_R1["ss"]] * len(cases), ifprec=2) as b:
+        assert b.solve(epscg=1e-10) == [0] * len(cases)
+        ncg0 = [i.ncg for i in b.infos]
+        x0 = b.solution(1)
+        b.set_guess(1, x0)  # the converged solution as the guess: almost nothing to do
+        assert b.solve(epscg=1e-10) == [0] * len(cases)
+        assert b.infos[1].ncg < ncg0[1] // 2
+        assert np.linalg.norm(b.solution(1) - x0) <= 1e-9 * np.linalg.norm(x0)
+        b.set_guess(1, None)
+        assert b.solve(epscg=1e-10) == [0] * len(cases)
+        assert [i.ncg for i in b.infos] == ncg0
+        with pytest.raises(ValueError):
+            b.set_guess(0, np.zeros(3))

@@ -77,7 +77,7 @@ def _legacy():
     return L.load_external_lu_solver, L.external_lu_solver, L.unload_external_lu_solver
 
 
-@pytest.mark.parametrize("dims", [(12, 11, 14), (30, 21, 17)])
+@pytest.mark.parametrize("dims", [(12, 11, 14), (30, 21, 17), (63, 91, 181)])
 def test_legacy_external_lu_solver(cuda, dims):
     """load/external/unload_external_lu_solver on device CSR arrays built by
     the oracle's getM/diacsr, as the -DCUSPARSE Fortran host passes them."""
@@ -103,3 +103,65 @@ def test_legacy_external_lu_solver(cuda, dims):
             apply_(C.c_void_p(xt.data_ptr()))
             assert np.array_equal(xt.cpu().numpy(), o.prec(x))
         unload()
+
+
+def _apply(load, apply_, unload, ia, ja, a, N, rhs, cuda):
+    import torch
+    ia_d = torch.tensor(ia, dtype=torch.int32, device=cuda)
+    ja_d = torch.tensor(ja, dtype=torch.int32, device=cuda)
+    a_d = torch.tensor(a, dtype=torch.float32, device=cuda)
+    torch.cuda.synchronize()
+    load(C.c_void_p(a_d.data_ptr()), C.c_void_p(ia_d.data_ptr()), C.c_void_p(ja_d.data_ptr()), N, int(ia[-1]))
+    xt = torch.tensor(rhs, device=cuda)
+    apply_(C.c_void_p(xt.data_ptr()))
+    z = xt.cpu().numpy()
+    unload()
+    return z
+
+
+def _lusol_np(ia, ja, lu, x):
+    """lusol (src/pot3d.F90:5227-5302) on a general factored 1-based CSR in
+    FP32, one rounding per operation; dinv = real(1/d in FP64, REAL32)."""
+    N = ia.size - 1
+    y = x.astype(np.float32)
+    f = np.float32
+    diag = [int(np.nonzero(ja[ia[i] - 1:ia[i + 1] - 1] == i + 1)[0][0]) + ia[i] - 1 for i in range(N)]
+    for i in range(N):
+        v = y[i]
+        for k in range(ia[i] - 1, diag[i]):
+            v = f(v - f(lu[k] * y[ja[k] - 1]))
+        y[i] = v
+    for i in range(N - 1, -1, -1):
+        v = y[i]
+        for k in range(diag[i] + 1, ia[i + 1] - 1):
+            v = f(v - f(lu[k] * y[ja[k] - 1]))
+        y[i] = f(v * np.float32(1.0 / np.float64(lu[diag[i]])))
+    return y.astype(np.float64)
+
+
+def test_legacy_general_pattern_uses_the_level_route(cuda):
+    """A CSR without the 7-point pattern (random structurally symmetric,
+    diagonally dominant) goes through the level-scheduled sweeps; the
+    factor is ilu0's and the solve lusol's, bit for bit."""
+    rng = np.random.default_rng(9)
+    N = 300
+    rows = [set([i]) for i in range(N)]
+    for _ in range(4 * N):
+        i, j = rng.integers(N, size=2)
+        rows[i].add(int(j))
+        rows[j].add(int(i))
+    ia, ja, a = [1], [], []
+    for i in range(N):
+        cols = sorted(rows[i])
+        for j in cols:
+            ja.append(j + 1)
+            a.append(float(len(cols) + 1) if j == i else float(rng.uniform(-1, 0)))
+        ia.append(len(ja) + 1)
+    ia = np.array(ia, np.int32)
+    ja = np.array(ja, np.int32)
+    a = np.array(a, np.float32)
+    f_ref, icode = O.ilu0_csr(ia, ja, a)
+    assert icode == 0
+    rhs = rng.standard_normal(N)
+    z = _apply(*_legacy(), ia, ja, a, N, rhs, cuda)
+    assert np.array_equal(z, _lusol_np(ia, ja, f_ref, rhs))

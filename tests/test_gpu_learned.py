@@ -1,0 +1,54 @@
+"""What the trained network gains (the learned warm start, hook
+x_cg(:) = 0 of src/pot3d.F90:3924): the committed operator for the
+127x181x361 PFSS grid predicts the initial guess of two seeds it never saw
+(training seeds 1000-2999, these 5000 and 5001), and the solver -- ILU(0),
+FP32-inner / FP64-refined -- reaches epsn 1e-9 from that guess in clearly
+fewer iterations than from zero, while PCG, not the network, decides
+convergence: solved to 1e-11 from either start the solutions agree to
+1e-8 relative L2.  The 200-seed evaluation of the same operator is recorded
+in pot3d_b200/weights/fno_pfss_127x181x361.json."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from pot3d_b200 import host
+from pot3d_b200.solver import Pot3dSolver
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+WEIGHTS = os.path.join(ROOT, "pot3d_b200", "weights", "fno_pfss_127x181x361")
+MAX_ITERATION_RATIO = 0.92  # at least 8% fewer iterations from the guess, per seed
+
+
+@pytest.mark.parametrize("seed", [5000, 5001])
+def test_learned_guess_cuts_iterations_on_held_out_seeds(cuda, seed):
+    import torch
+    from pot3d_b200.fno import FNO, grid_from_mesh
+    from pot3d_b200.tc import check_errors
+    from pot3d_b200.warmstart import Inputs, case_br0
+    mesh = host.make_mesh(127, 181, 361)
+    model = FNO.load(WEIGHTS + ".npz", grid_from_mesh(mesh))
+    inputs = Inputs(model)
+    br0 = case_br0(mesh, seed, 40, 20)
+    v, sig = inputs.normalized(br0)
+    with Pot3dSolver(mesh, br0, ifprec=2, precision="fp32_refined") as s:
+        b = torch.tensor(s.rhs(), device=cuda)
+        guess = model.predict(inputs.build(torch.from_numpy(v).cuda().view(1, -1)), [sig])[0]
+        check_errors()
+        res = {}
+        for start in ("zero", "guess"):
+            for eps in (1e-9, 1e-11):
+                x = torch.zeros_like(b) if start == "zero" else guess.clone()
+                r = b.clone()
+                assert s.cgsolve_dev(x, r, epscg=eps, ncgmax=20000) == 0
+                res[start, eps] = (s.last_info.ncg, x.cpu().numpy())
+    n0, n1 = res["zero", 1e-9][0], res["guess", 1e-9][0]
+    assert n1 <= MAX_ITERATION_RATIO * n0, (n1, n0)
+    xa, xb = res["zero", 1e-11][1], res["guess", 1e-11][1]
+    assert np.linalg.norm(xb - xa) <= 1e-8 * np.linalg.norm(xa)
+    # the guess is close but not the answer: the solve still does the work
+    err = np.linalg.norm(guess.cpu().numpy() - xa) / np.linalg.norm(xa)
+    assert 1e-6 < err < 0.05, err
