@@ -520,58 +520,65 @@ def main():
                 "k_update": {"ms": ms[1], "bytes": by[1], "gbs": by[1] / (ms[1] * 1e-3) / 1e9}}
 
     # FP64 PCG beside it: ILU(0) from zero (same preconditioner) and the
-    # diagonal preconditioner (the reference's default), same inputs.
-    plain = same_prec = None
-    s64 = None
+    # diagonal preconditioner (the reference's default), same inputs.  One
+    # FP64 solver at a time besides the headline one (the largest workload
+    # needs ~70 GB per solver).
+    plain = same_prec = parity = None
     if not args.no_plain or not args.no_parity:
         s64 = Pot3dSolver(mesh, br0, option=opt, ifprec=2, precision="fp64", device=local)
+        if not args.no_plain:
+            r64 = [solve_resident(s64, learned=False) for _ in range(2 if args.warmup > 0 else 1)]
+            if any(q["ierr"] for q in r64):
+                raise SystemExit("the FP64 ILU(0) solve did not converge")
+            t64 = reduce_max(r64[-1]["seconds"], ws)
+            same_prec = {"seconds": t64, "iterations": r64[-1]["ncg"], "ifprec": 2, "precision": "fp64",
+                         "initial_guess": "zero", "speedup": t64 / t_dev}
+        if not args.no_parity:
+            # Parity: the headline method and FP64 PCG both to 1e-11; the timed
+            # 1e-9 solution against the FP64 1e-11 one; against the oracle's.
+            def fields(x):
+                out = s.fields(x, want=("phi", "w"))
+                return out["phi"], out["w"]
+            ref = solve_resident(s64, learned=False, epscg=1e-11)
+            x64 = xt.cpu().numpy()
+            mine = solve_resident(s, learned=True, epscg=1e-11)
+            x11 = xt.cpu().numpy()
+            phi64, w64 = fields(x64)
+            del x64
+            phi11, w11 = fields(x11)
+            del x11
+            parity = {"epscg": 1e-11, "fp64_ilu_iterations": ref["ncg"], "method_iterations": mine["ncg"],
+                      "phi_rel_l2": rel_l2(phi11, phi64),
+                      "energy_rel_err": float(np.max(np.abs(w11 - w64) / np.abs(w64)))}
+            phi9, w9 = fields(x_timed)
+            parity["timed_1e-9_phi_rel_l2"] = rel_l2(phi9, phi64)
+            parity["timed_1e-9_energy_rel_err"] = float(np.max(np.abs(w9 - w64) / np.abs(w64)))
+            parity["energies_1e-11"] = w11.tolist()
+            del phi9, phi64
+            parity["oracle"] = {}
+            for pf in (2, 1):
+                fix = oracle_fixture(args.workload, pf) if rank == 0 else None
+                if fix is None:
+                    continue
+                wo = np.asarray(fix["energy"])
+                sl = np.stack([phi11[i - 1, ::fix["stride"], ::fix["stride"]] for i in fix["slice_i"]])
+                parity["oracle"][f"ifprec{pf}"] = {
+                    "source": f"tests/golden/{args.workload}_oracle_ifprec{pf} (oracle FP64 PCG to 1e-11, "
+                              f"{fix['iterations']} iterations)",
+                    "energy_rel_err": float(np.max(np.abs(w11 - wo) / np.abs(wo))),
+                    "phi_slices_rel_l2": rel_l2(sl, fix["phi_slices"])}
+            del phi11
+        s64.close()
     if not args.no_plain:
-        r64 = [solve_resident(s64, learned=False) for _ in range(2 if args.warmup > 0 else 1)]
-        same_prec = {"seconds": reduce_max(r64[-1]["seconds"], ws), "iterations": r64[-1]["ncg"], "ifprec": 2,
-                     "precision": "fp64", "initial_guess": "zero", "speedup": reduce_max(r64[-1]["seconds"], ws) / t_dev}
         sp = Pot3dSolver(mesh, br0, option=opt, ifprec=1, precision="fp64", device=local)
         pt = [solve_resident(sp, learned=False) for _ in range(2 if args.warmup > 0 else 1)]
         sp.close()
-        if any(q["ierr"] for q in pt + r64):
-            raise SystemExit("an FP64 solve did not converge")
+        if any(q["ierr"] for q in pt):
+            raise SystemExit("the plain FP64 solve did not converge")
         t_plain = reduce_max(pt[-1]["seconds"], ws)
         plain = {"seconds": t_plain, "iterations": pt[-1]["ncg"], "ifprec": 1, "precision": "fp64",
                  "initial_guess": "zero", "speedup": t_plain / t_dev,
                  "achieved_gbs": 80.0 * N * pt[-1]["ncg"] / t_plain / 1e9}
-
-    # Parity: the headline method and FP64 PCG both to 1e-11; the timed 1e-9
-    # solution against the FP64 1e-11 one; energies against the oracle's.
-    parity = None
-    if not args.no_parity:
-        def fields(x):
-            out = s.fields(x, want=("phi", "w"))
-            return out["phi"], out["w"]
-        ref = solve_resident(s64, learned=False, epscg=1e-11)
-        x64 = xt.cpu().numpy()
-        mine = solve_resident(s, learned=True, epscg=1e-11)
-        x11 = xt.cpu().numpy()
-        phi64, w64 = fields(x64)
-        phi11, w11 = fields(x11)
-        phi9, w9 = fields(x_timed)
-        parity = {"epscg": 1e-11, "fp64_ilu_iterations": ref["ncg"], "method_iterations": mine["ncg"],
-                  "phi_rel_l2": rel_l2(phi11, phi64), "energy_rel_err": float(np.max(np.abs(w11 - w64) / np.abs(w64))),
-                  "timed_1e-9_phi_rel_l2": rel_l2(phi9, phi64),
-                  "timed_1e-9_energy_rel_err": float(np.max(np.abs(w9 - w64) / np.abs(w64))),
-                  "energies_1e-11": w11.tolist()}
-        parity["oracle"] = {}
-        for pf in (2, 1):
-            fix = oracle_fixture(args.workload, pf) if rank == 0 else None
-            if fix is None:
-                continue
-            wo = np.asarray(fix["energy"])
-            sl = np.stack([phi11[i - 1, ::fix["stride"], ::fix["stride"]] for i in fix["slice_i"]])
-            parity["oracle"][f"ifprec{pf}"] = {
-                "source": f"tests/golden/{args.workload}_oracle_ifprec{pf} (oracle FP64 PCG to 1e-11, "
-                          f"{fix['iterations']} iterations)",
-                "energy_rel_err": float(np.max(np.abs(w11 - wo) / np.abs(wo))),
-                "phi_slices_rel_l2": rel_l2(sl, fix["phi_slices"])}
-    if s64 is not None:
-        s64.close()
 
     if rank != 0:
         s.close()

@@ -273,6 +273,12 @@ int pot3d_gpu_batch_set_guess(pot3d_gpu_batch *b, int i, const double *x);
  * block, keeps the fastest (*best_tk; ms_out[c] = time of candidate c). */
 int pot3d_gpu_batch_tune(pot3d_gpu_batch *b, const int *candidates, int ncand, int iters, int *best_tk,
                          float *ms_out);
+/* Autotuner over two tile parameters: the stencil's planes per block
+ * (cand_tk, 8..512) and the update kernels' planes per block (cand_tku, >=
+ * 8); times every pair, keeps the fastest; ms_out[c * n_tku + d] = time of
+ * (cand_tk[c], cand_tku[d]). */
+int pot3d_gpu_batch_tune2(pot3d_gpu_batch *b, const int *cand_tk, int n_tk, const int *cand_tku, int n_tku,
+                          int iters, int *best_tk, int *best_tku, float *ms_out);
 /* Solve all cases from their guesses (x = 0 unless set) to epscg (ernorm's
  * rule per case; with FP32_REFINED, info[i].n_refine the case's reliable
  * updates); ierr[i],

@@ -20,7 +20,7 @@ GPU_SYMBOLS = (
     "pot3d_gpu_create", "pot3d_gpu_destroy", "pot3d_gpu_size", "pot3d_gpu_rhs", "pot3d_gpu_cgsolve",
     "pot3d_gpu_cgsolve_dev", "pot3d_gpu_history", "pot3d_gpu_finalize_phi", "pot3d_gpu_energy", "pot3d_gpu_fields",
     "pot3d_gpu_ax_dev", "pot3d_gpu_prec_dev", "pot3d_gpu_precond_diag", "pot3d_gpu_last_error",
-    "pot3d_gpu_time_kernels", "pot3d_gpu_time_sweeps", "pot3d_gpu_set_refine", "pot3d_gpu_refine_info", "pot3d_gpu_test_sweep_stall", "pot3d_gpu_set_br0", "pot3d_gpu_br0_from_map", "pot3d_gpu_batch_create", "pot3d_gpu_batch_create_ex", "pot3d_gpu_batch_create_mode", "pot3d_gpu_batch_set_guess", "pot3d_gpu_batch_tune", "pot3d_gpu_batch_solve",
+    "pot3d_gpu_time_kernels", "pot3d_gpu_time_sweeps", "pot3d_gpu_set_refine", "pot3d_gpu_refine_info", "pot3d_gpu_test_sweep_stall", "pot3d_gpu_set_br0", "pot3d_gpu_br0_from_map", "pot3d_gpu_batch_create", "pot3d_gpu_batch_create_ex", "pot3d_gpu_batch_create_mode", "pot3d_gpu_batch_set_guess", "pot3d_gpu_batch_tune2", "pot3d_gpu_batch_tune", "pot3d_gpu_batch_solve",
     "pot3d_gpu_batch_solution", "pot3d_gpu_batch_destroy",
 )
 HOST_SYMBOLS = ("pot3d_host_genmesh", "pot3d_host_mesh", "pot3d_host_br0", "pot3d_host_synthetic_br")
@@ -86,6 +86,7 @@ def lib():
         L.pot3d_gpu_batch_create_mode.argtypes = [C.c_int, C.POINTER(MeshC), C.POINTER(dp), dp, C.c_int, C.c_int,
                                                   C.c_int, C.POINTER(vp)]
         L.pot3d_gpu_batch_set_guess.argtypes = [vp, C.c_int, dp]
+        L.pot3d_gpu_batch_tune2.argtypes = [vp, ip, C.c_int, ip, C.c_int, C.c_int, ip, ip, fp]
         L.pot3d_gpu_batch_tune.argtypes = [vp, ip, C.c_int, C.c_int, ip, fp]
         L.pot3d_gpu_batch_solve.argtypes = [vp, C.c_int, C.c_double, ip, C.POINTER(SolveInfo), dp]
         L.pot3d_gpu_batch_solution.argtypes = [vp, C.c_int, dp]

@@ -75,8 +75,9 @@ def main(argv=None):
            "map": {"lmax": LMAX, "bipoles": NBIP}, "specs": specs}
     with BatchSolver(meshes, brs, [PM_R1["ss"]] * a.n, ifprec=a.ifprec, precision=a.precision) as b:
         t0 = time.perf_counter()
-        best, times = b.tune()
-        rep["tune"] = {"best_planes_per_block": best, "ms": times, "seconds": time.perf_counter() - t0}
+        (best, best_u), times = b.tune2()
+        rep["tune"] = {"best_planes_per_block": best, "best_update_planes_per_block": best_u,
+                       "ms": {f"{k[0]}x{k[1]}": v for k, v in times.items()}, "seconds": time.perf_counter() - t0}
         secs = []
         for _ in range(a.repeats):
             ierr = b.solve(epscg=a.epscg)

@@ -1146,7 +1146,18 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
     int dev = 0, nsm = 148, occ_s = 2, occ_u = 8;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_stencil<MODE_PCG>, NTHR, StageLayout<MODE_PCG>::smem));
+    // occupancy of the stencil form this solver iterates with (the ILU(0)
+    // forms hold three blocks per SM, the diagonal ones two)
+    if (ifprec == 2 && precision == POT3D_FP32_REFINED)
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_stencil<MODE_PCGZ32>, NTHR,
+                                                       StageLayout<MODE_PCGZ32>::smem));
+    else if (ifprec == 2)
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_stencil<MODE_PCGZ>, NTHR, StageLayout<MODE_PCGZ>::smem));
+    else if (precision == POT3D_FP32_REFINED)
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_stencil<MODE_PCG32>, NTHR,
+                                                       StageLayout<MODE_PCG32>::smem));
+    else
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_stencil<MODE_PCG>, NTHR, StageLayout<MODE_PCG>::smem));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k_update<UPD_ITER, false>, NTHR, 0));
     const long long cols = (long long)g.nit * g.njt;
     auto pick = [&](int slots_per_sm, double startup, int max_tk, int *tk, int *nkc) {
@@ -1985,6 +1996,7 @@ struct Batch {
   std::vector<int> graph_act;  // the table the graph was captured for
   int U = 8;
   int tk = 0;      // stencil planes per block (0 = per-case default)
+  int tku = 0;     // update kernels' planes per block (0 = per-case default)
   int ifprec = 1;  // 1: diagonal preconditioner; 2: ILU(0) with batched wavefront sweeps
   int precision = POT3D_FP64;  // or POT3D_FP32_REFINED: FP32-inner iterations, per-case reliable updates
   DiluBatch *wave = nullptr;
@@ -2024,6 +2036,23 @@ static void batch_set_tk(Batch &B, int tk) {
     }
   }
   B.tk = tk;
+}
+
+// The same for the update kernels' planes per block (0 = per-case default).
+// Their ring partials and reduction slots are sized at creation for any
+// value >= 8.
+static void batch_set_tku(Batch &B, int tku) {
+  for (Solver *sp : B.inst) {
+    Solver &s = *sp;
+    if (tku > 0) {
+      s.g.tk_u = std::min(tku, s.g.npm2);
+      s.g.nkc_u = (s.g.npm2 + s.g.tk_u - 1) / s.g.tk_u;
+    } else {
+      s.g.tk_u = s.tku_default;
+      s.g.nkc_u = s.nkcu_default;
+    }
+  }
+  B.tku = tku;
 }
 
 // Build and upload the instance table of the cases in B.act.
@@ -2306,10 +2335,15 @@ extern "C" int pot3d_gpu_batch_create_mode(int n, const pot3d_mesh_t *meshes, co
     if (!st) {
       s->tk_default = s->g.tk;
       s->nkc_default = s->g.nkc;
-      // reduction slots of the stencil for any planes per block >= 8
-      const size_t need = (size_t)s->g.nit * s->g.njt * ((s->g.npm2 + 7) / 8);
+      s->tku_default = s->g.tk_u;
+      s->nkcu_default = s->g.nkc_u;
+      // reduction slots and south-ring partials for any planes per block >= 8
+      const size_t chunks = (size_t)(s->g.npm2 + 7) / 8;
+      const size_t need = (size_t)s->g.nit * s->g.njt * chunks;
       if (need > std::max<size_t>(s->nblk_tiled, 148 * 16 * 3))
         st = s->alloc((void **)&s->d_partials, sizeof(double) * need);
+      if (!st && chunks > (size_t)s->g.nkc_u)
+        st = s->alloc((void **)&s->d_s1z, sizeof(double) * chunks * s->g.NRP);
     }
   }
   // the cases' setup ran on their own streams; from now on they run on the batch's
@@ -2378,6 +2412,50 @@ extern "C" int pot3d_gpu_batch_set_guess(pot3d_gpu_batch *h, int i, const double
 
 // Autotuner: times `iters` batched iterations of all cases for each candidate
 // planes per block; applies and returns the fastest.
+extern "C" int pot3d_gpu_batch_tune2(pot3d_gpu_batch *h, const int *cand_tk, int n_tk, const int *cand_tku, int n_tku,
+                                     int iters, int *best_tk, int *best_tku, float *ms_out) {
+  using namespace pot3d;
+  if (!h || !cand_tk || n_tk < 1 || !cand_tku || n_tku < 1 || iters < 1) {
+    pot3d_set_error("pot3d_gpu_batch_tune2: invalid arguments");
+    return POT3D_ERR_ARG;
+  }
+  Batch &B = h->b;
+  for (int c = 0; c < n_tk; c++)
+    if (cand_tk[c] < 8 || cand_tk[c] > MAX_TK) {
+      pot3d_set_error("pot3d_gpu_batch_tune2: stencil planes per block must be in [8, 512]");
+      return POT3D_ERR_ARG;
+    }
+  for (int c = 0; c < n_tku; c++)
+    if (cand_tku[c] < 8) {
+      pot3d_set_error("pot3d_gpu_batch_tune2: update planes per block must be at least 8");
+      return POT3D_ERR_ARG;
+    }
+  float best = 1e30f;
+  int bt = cand_tk[0], btu = cand_tku[0], st;
+  B.act.resize(B.inst.size());
+  for (size_t q = 0; q < B.inst.size(); q++) B.act[q] = (int)q;
+  for (int c = 0; c < n_tk; c++)
+    for (int d = 0; d < n_tku; d++) {
+      batch_set_tk(B, cand_tk[c]);
+      batch_set_tku(B, cand_tku[d]);
+      if ((st = batch_table(B))) return st;
+      float ms = 0.f;
+      if ((st = batch_time(B, iters, &ms))) return st;
+      if (ms_out) ms_out[c * n_tku + d] = ms;
+      if (ms < best) {
+        best = ms;
+        bt = cand_tk[c];
+        btu = cand_tku[d];
+      }
+    }
+  batch_set_tk(B, bt);
+  batch_set_tku(B, btu);
+  B.graph_act.clear();  // the graph (if any) belongs to another tiling
+  if (best_tk) *best_tk = bt;
+  if (best_tku) *best_tku = btu;
+  return POT3D_OK;
+}
+
 extern "C" int pot3d_gpu_batch_tune(pot3d_gpu_batch *h, const int *candidates, int ncand, int iters, int *best_tk,
                                     float *ms_out) {
   using namespace pot3d;

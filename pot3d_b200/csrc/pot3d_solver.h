@@ -28,6 +28,7 @@ struct Solver {
   double *d_partials = nullptr;
   size_t nblk_tiled = 0;
   int tk_default = 0, nkc_default = 0;  // stencil k-chunking chosen at setup
+  int tku_default = 0, nkcu_default = 0;  // the update kernels' k-chunking
   double *d_s1z = nullptr, *d_s1p = nullptr, *d_s1 = nullptr;
   double *d_scalar = nullptr, *d_sums = nullptr, *d_hist = nullptr;
   int hist_cap = 0;

@@ -282,6 +282,21 @@ class BatchSolver:
         self.tk = best.value
         return best.value, {int(k): float(v) for k, v in zip(candidates, ms)}
 
+    def tune2(self, candidates=(16, 32, 48, 64), update_candidates=(16, 32, 64, 128), iters: int = 6):
+        """Pick the stencil's and the update kernels' planes per block
+        together by timing every pair; returns ((best, best_update),
+        {(candidate, update_candidate): ms})."""
+        c = (C.c_int * len(candidates))(*candidates)
+        d = (C.c_int * len(update_candidates))(*update_candidates)
+        ms = (C.c_float * (len(candidates) * len(update_candidates)))()
+        b, bu = C.c_int(0), C.c_int(0)
+        check(_lib.lib().pot3d_gpu_batch_tune2(self._h, c, len(candidates), d, len(update_candidates), iters,
+                                               C.byref(b), C.byref(bu), ms))
+        self.tk = b.value
+        times = {(int(x), int(y)): float(ms[i * len(update_candidates) + j])
+                 for i, x in enumerate(candidates) for j, y in enumerate(update_candidates)}
+        return (b.value, bu.value), times
+
     def solve(self, epscg: float = 1e-9, ncgmax: int = 10_000_000):
         """Solve every case; returns the list of ierr (0 = converged)."""
         ierr = (C.c_int * self.n)()
