@@ -56,11 +56,23 @@ METRIC = "solve s to 1e-9 resid: learned+FP32-refined vs plain FP64 PCG on 1 B20
 # touched once per fused pass): FP64 PCG iteration 80 (ifprec=1) / 104
 # (ifprec=2); FP32-inner iteration 40 / 64; each FP64 reliable update 24.
 # The ILU(0) application moves 12 B forward (r32, d, y) and 12 B backward
-# (y, d, z32).
+# (y, d, z32).  In the refined mode's inner iteration the forward sweep also
+# applies the residual half of the update (q32 read, r32 written: +8 B; its
+# r32 read is the sweep's own) and the backward sweep forms rho from the y
+# and d it reads (no bytes).
 BYTES_PER_UNKNOWN_ITER = {("fp64", 1): 80.0, ("fp64", 2): 104.0, ("fp32_refined", 1): 40.0,
                           ("fp32_refined", 2): 64.0}
 BYTES_PER_REFINE = 24.0
-SWEEP_BYTES_PER_UNKNOWN = {"k_dilu_wave<fwd>": 12.0, "k_dilu_wave<bwd>": 12.0}
+SWEEP_BYTES_PER_UNKNOWN = {"k_dilu_wave<fwd>": 12.0, "k_dilu_wave<bwd>": 12.0,
+                           "k_dilu_wave<fwd,fused>": 20.0, "k_dilu_wave<bwd,fused>": 12.0}
+
+
+def sweep_names(precision: str):
+    """The sweep kernels a solver of this arithmetic iterates with (what
+    pot3d_gpu_time_sweeps times)."""
+    if precision == "fp32_refined":
+        return ("k_dilu_wave<fwd,fused>", "k_dilu_wave<bwd,fused>")
+    return ("k_dilu_wave<fwd>", "k_dilu_wave<bwd>")
 FALLBACK_HBM_GBS = 6650.0
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
@@ -401,7 +413,7 @@ def main():
         if args.ifprec == 2:
             fms, bms = s.time_sweeps(2)
             out = {}
-            for name, t in (("k_dilu_wave<fwd>", fms), ("k_dilu_wave<bwd>", bms)):
+            for name, t in zip(sweep_names(args.precision), (fms, bms)):
                 by = SWEEP_BYTES_PER_UNKNOWN[name] * s.N
                 out[name] = {"ms": t, "gbs": by / (t * 1e-3) / 1e9}
             print(json.dumps({"workload": args.workload, "kernels": out}))
@@ -511,7 +523,7 @@ def main():
     if args.ifprec == 2:
         fms, bms = s.time_sweeps(10)
         kern = {}
-        for name, t in (("k_dilu_wave<fwd>", fms), ("k_dilu_wave<bwd>", bms)):
+        for name, t in zip(sweep_names(args.precision), (fms, bms)):
             by = SWEEP_BYTES_PER_UNKNOWN[name] * N
             kern[name] = {"ms": t, "bytes": by, "gbs": by / (t * 1e-3) / 1e9}
     elif args.precision == "fp64":

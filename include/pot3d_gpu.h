@@ -210,9 +210,11 @@ int pot3d_gpu_precond_diag(pot3d_gpu_solver *s, float *d, float *dinv);
  * update: x, p, r, Ap read, x, r written; 8 B each per unknown). */
 int pot3d_gpu_time_kernels(pot3d_gpu_solver *s, int reps, double ms[2], double bytes[2]);
 /* Average device milliseconds of the ILU(0) forward (ms[0]) and backward
- * (ms[1]) wavefront sweeps over `reps` applications (ifprec = 2 only).
- * No counterpart in the reference (its timers cover whole preconditioner
- * calls, src/pot3d.F90 timing.out "PC"). */
+ * (ms[1]) wavefront sweeps over `reps` applications (ifprec = 2 only), in
+ * the form the solver iterates with: the plain sweeps for FP64 PCG, the
+ * sweeps fused with the inner update's residual half and with rho for the
+ * refined mode.  No counterpart in the reference (its timers cover whole
+ * preconditioner calls, src/pot3d.F90 timing.out "PC"). */
 int pot3d_gpu_time_sweeps(pot3d_gpu_solver *s, int reps, double ms[2]);
 
 /* Failure-detection check of the ILU(0) wavefront sweeps (ifprec = 2): runs

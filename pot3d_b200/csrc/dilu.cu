@@ -196,6 +196,9 @@ struct WaveArgs {
                          // failure-detection test uses it to make its consumers' waits run out
   int nte, ntj, ntiles, ndiag, nsteps;
   int pad;               // nsteps - (npm2 + WSK): idle steps, trailing forward, leading backward
+  // Fused forms (the FP32-inner iteration of the refined mode):
+  float4 *rs;            // forward: the FP32 recurrence residual in the stream layout, read and rewritten
+  double *rz_part;       // backward: per-tile partial of rho = y.D^-1 y
 };
 
 __device__ __forceinline__ void wave_publish(unsigned long long *p, unsigned epoch, float v) {
@@ -220,8 +223,8 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 }
 
 struct alignas(128) WaveSmemF {      // forward sweep
-  float rin[WPG][WG][WJT][WE];       // r32 plane groups (TMA boxes), slot = plane group % WPG
-  float4 lf[WSL][3][WAVE_THREADS];   // coefficient groups
+  float rin[WPG][WG][WJT][WE];       // r32 (fused: q32) plane groups (TMA boxes), slot = plane group % WPG
+  float4 lf[WSL][4][WAVE_THREADS];   // coefficient groups (+ fused: the residual group)
   float y[2][WJT][WE + 1];           // step parity, line values
   float ring[WXR][2][WCH][16];       // chunk % WXR, face (0: e, 1: j), step in chunk, line
   uint64_t bar_s[WSL];                // one per stream slot, also counting the plane group of the step group
@@ -234,6 +237,7 @@ struct alignas(128) WaveSmemB {      // backward sweep
   float zout[WROUT][WAVE_THREADS];   // z32 planes [jl][el], slot = plane % WROUT (TMA store source)
   float y[2][WJT][WE + 1];
   float ring[WXR][2][WCH][16];
+  double red[WAVE_THREADS / 32];     // fused: the tile's rho partial, per compute warp
   uint64_t bar_s[WSL];
   int2 tile;
   // zflushed: z32 planes, from the top, whose TMA store has read its slot
@@ -381,7 +385,7 @@ __device__ __forceinline__ bool wave_mbar_wait(uint64_t *bar, uint32_t parity, c
 // the compute warps report the slot free (S.gdone = groups they finished).
 // No copy is issued on the compute warps' dependent path.  Before it
 // returns after an abort, lane 0 waits (bounded) for what it issued.
-template <bool FWD>
+template <bool FWD, bool FUSE = false>
 __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *map,
                                           typename WaveSmemSel<FWD>::type &S, const WaveFaces &f, int gbase,
                                           int qbase, bool acquire_map) {
@@ -408,9 +412,11 @@ __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *
         uint64_t *bar = &S.bar_s[slot];
         if constexpr (FWD) {
           const bool plane = ns < NQ;
-          mbar_expect_tx(bar, 3 * WAVE_THREADS * 16 + (plane ? WG * WJT * WE * 4 : 0));
+          mbar_expect_tx(bar, (FUSE ? 4 : 3) * WAVE_THREADS * 16 + (plane ? WG * WJT * WE * 4 : 0));
           bulk_load(&S.lf[slot][0][0], a.lf + ((size_t)ti * G + ns) * 3 * WAVE_THREADS, 3 * WAVE_THREADS * 16,
                     bar);
+          if (FUSE)  // the group's residual r32 (stream layout)
+            bulk_load(&S.lf[slot][3][0], a.rs + ((size_t)ti * G + ns) * WAVE_THREADS, WAVE_THREADS * 16, bar);
           if (plane)
             tma_load_3d(&S.rin[(qbase + ns) % WPG][0][0][0], map, f.te * WE, f.tj * WJT, ns * WG, bar);
         } else {
@@ -465,7 +471,7 @@ __device__ __forceinline__ void wave_copy(const WaveArgs &a, const CUtensorMap *
   if constexpr (!FWD) bulk_wait_all();  // the tile's z32 planes are in global memory
 }
 
-template <bool FWD>
+template <bool FWD, bool FUSE = false>
 __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
                                           typename WaveSmemSel<FWD>::type &S, const WaveFaces &f, unsigned epoch,
                                           int gbase, int qbase) {
@@ -506,6 +512,17 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
 
   float seam_y = 0.f;  // value at the line's first plane of the sweep
   float prev = 0.f;    // own value at the previous step
+  // Fused forward: the box ring holds q32, and the residual half of the
+  // inner update, r32 = r32 - alpha q rounded once, is formed from the
+  // streamed r32 of the step (the operations of the unfused update, so the
+  // values are the same) at the start of each step group, off the steps'
+  // dependent chain, and written back to the stream.  Fused backward:
+  // rho = y.D^-1 y, which equals r.M^-1 r for M = L (D + U) with L = I +
+  // E D^-1 and U = E^T (the D-ILU factors of the symmetric A), accumulated
+  // in FP64 from the y and dinv the sweep reads anyway.
+  double alpha = 0.0;
+  if constexpr (FUSE && FWD) alpha = *(const volatile double *)&a.st->alpha;
+  double rz = 0.0;
   // forward: plane p = t - sk of this line sits in slot (qbase + p / WG) % WPG,
   // row p % WG (p < 0 at the first steps: the entry is never read)
   int p_sub = 0, p_slot = 0;
@@ -560,6 +577,7 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         c0 = S.lf[sl][0][T];
         c1 = S.lf[sl][1][T];
         c2 = S.lf[sl][2][T];
+        if constexpr (FUSE) c3 = S.lf[sl][3][T];  // the group's residual r32
       } else {
         c0 = S.ub[sl][0][T];
         c1 = S.ub[sl][1][T];
@@ -567,7 +585,20 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         c3 = S.ub[sl][3][T];
         yin4 = S.yin[sl][T];
       }
-      float y4[WG];
+      float y4[WG], rn4[WG], vin4[WG];
+      if constexpr (FWD && FUSE) {
+        // every plane of the group's steps arrived with group gi's copies
+#pragma unroll
+        for (int u = 0; u < WG; u++) {
+          const float qv = S.rin[p_slot][p_sub][jl][el];
+          if (++p_sub == WG) {
+            p_sub = 0;
+            p_slot = p_slot + 1 == WPG ? 0 : p_slot + 1;
+          }
+          const float ro = u == 0 ? c3.x : u == 1 ? c3.y : u == 2 ? c3.z : c3.w;
+          vin4[u] = (float)fma(-alpha, (double)qv, (double)ro);  // r32 - alpha q
+        }
+      }
 #pragma unroll
       for (int u = 0; u < WG; u++) {
         const int t = gi * WG + u;
@@ -579,7 +610,9 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         const float k3 = u == 0 ? c3.x : u == 1 ? c3.y : u == 2 ? c3.z : c3.w;
         // backward y: forward step nsteps-1-t, component 3-u of the group
         float v_in = u == 0 ? yin4.w : u == 1 ? yin4.z : u == 2 ? yin4.y : yin4.x;
-        if constexpr (FWD) {
+        if constexpr (FWD && FUSE) {
+          v_in = vin4[u];
+        } else if constexpr (FWD) {
           v_in = S.rin[p_slot][p_sub][jl][el];
           if (++p_sub == WG) {
             p_sub = 0;
@@ -609,6 +642,7 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
           y = __fsub_rn(y, __fmul_rn(k2, ne));
           y = act ? y : 0.f;
           seam_y = (act && kk == 0) ? y : seam_y;
+          rn4[u] = act ? v_in : 0.f;
         } else {
           // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv; u_k = 0 on the last plane
           const float ks = kk == 0 ? seam_c : 0.f;
@@ -620,6 +654,11 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
           y = act ? y : 0.f;
           seam_y = (act && kk == npm2 - 1) ? y : seam_y;
           if (act) S.zout[kk % WROUT][T] = y;
+          if constexpr (FUSE) {
+            // y and dinv are exact zeros where the thread has no point
+            const double yv = (double)v_in;
+            rz = fma(yv * (double)k3, yv, rz);
+          }
         }
         S.y[t & 1][jl][el] = y;
         if (pub_e && act) wave_publish(xe_out + (size_t)t * 16, epoch, y);
@@ -638,6 +677,8 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         }
       }
       if constexpr (FWD) a.ys[((size_t)ti * G + gi) * WAVE_THREADS + T] = make_float4(y4[0], y4[1], y4[2], y4[3]);
+      if constexpr (FWD && FUSE)
+        a.rs[((size_t)ti * G + gi) * WAVE_THREADS + T] = make_float4(rn4[0], rn4[1], rn4[2], rn4[3]);
     }
     if (T == 0) *(volatile int *)&S.consumed = c + 1;
   }
@@ -645,11 +686,26 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
     __threadfence_block();
     *(volatile int *)&S.gdone = G;
   }
+  if constexpr (FUSE && !FWD) {  // the tile's rho partial, in a fixed order
+    const double w = warp_sum(rz);
+    if ((T & 31) == 0) S.red[T >> 5] = w;
+    wave_bar_compute();
+    if (T == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < WAVE_THREADS / 32; q++) t += S.red[q];
+      a.rz_part[ti] = t;
+    }
+  }
   return true;
 }
 
-template <bool FWD>
-// map: forward, the r32 load map; backward, the z32 store map.
+// map: forward, the r32 load map (FUSE: q32); backward, the z32 store map.
+// FUSE: the forms of the FP32-inner iteration of the refined mode (see
+// wave_tile); the backward's last block then ends the iteration as the r.z
+// update would: the tiles' partials summed in tile order, rho, beta, ncg and
+// ernorm (rz_epilogue).
+template <bool FWD, bool FUSE = false>
 __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_constant__ CUtensorMap map,
                                                                     WaveArgs a) {
   using Sm = typename WaveSmemSel<FWD>::type;
@@ -685,9 +741,9 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
     if (role == 1)
       wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
     else if (role == 2)
-      wave_copy<FWD>(a, &map, S, f, gbase, qbase, false);
+      wave_copy<FWD, FUSE>(a, &map, S, f, gbase, qbase, false);
     else
-      ok = wave_tile<FWD>(a, S, f, epoch, gbase, qbase);
+      ok = wave_tile<FWD, FUSE>(a, S, f, epoch, gbase, qbase);
     if (!ok) S.abort = 1;
     __syncthreads();
     if (S.abort) {
@@ -701,13 +757,27 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
     qbase += FWD ? NQ : 0;
   }
   __syncthreads();
+  __shared__ int last;
   if (threadIdx.x == 0) {
     __threadfence();
-    if (atomicAdd(&a.ctl->done, 1u) == gridDim.x - 1) {  // last block: reset for the next sweep
+    last = atomicAdd(&a.ctl->done, 1u) == gridDim.x - 1;
+    if (last) {  // last block: reset for the next sweep
       atomicExch(&a.ctl->ticket, 0u);
       atomicExch(&a.ctl->done, 0u);
       __threadfence();
       atomicAdd(&a.ctl->epoch, 1u);
+    }
+  }
+  if constexpr (FUSE && !FWD) {
+    __syncthreads();
+    // every tile's partial is written (each block fenced before its count);
+    // in a solve (check) that is still running, end the iteration
+    if (last && run && a.check && threadIdx.x < 32) {
+      __threadfence();
+      double t = 0.0;
+      for (int q = threadIdx.x; q < a.ntiles; q += 32) t += __ldcg(a.rz_part + q);
+      t = warp_sum(t);
+      if (threadIdx.x == 0 && *(volatile int *)&a.st->status == ST_RUNNING) rz_epilogue<UPD_ZDOT>(a.st, t);
     }
   }
 }
@@ -936,6 +1006,33 @@ __global__ void k_wave_seam(Geo g, DevMesh m, const float *__restrict__ d, float
   }
 }
 
+// r32 (padded layout) into the fused forward's residual stream, in the
+// tile-skewed group layout of the coefficient streams; zero where a thread
+// has no point at a step.
+__global__ void k_wave_r_stream(Geo g, const float *__restrict__ r32, int nte, int ntiles, int nsteps,
+                                float4 *__restrict__ rs) {
+  const int G = nsteps / WG;
+  const long long total = (long long)ntiles * G * WAVE_THREADS;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int T = (int)(q % WAVE_THREADS);
+    const long long rr = q / WAVE_THREADS;
+    const int gi = (int)(rr % G);
+    const int ti = (int)(rr / G);
+    const int te = ti % nte, tj = ti / nte;
+    const int el = T & (WE - 1), jl = T / WE;
+    const int e = te * WE + el, jj = tj * WJT + jl;
+    const bool valid = e < g.nrm2 && jj < g.ntm2;
+    float v[WG];
+#pragma unroll
+    for (int s = 0; s < WG; s++) {
+      const int kf = gi * WG + s - (el + jl);
+      v[s] = (valid && kf >= 0 && kf < g.npm2) ? r32[g.idx(e, jj, kf)] : 0.f;
+    }
+    rs[q] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
 __global__ void k_narrow_rhs(long long n, const double *__restrict__ b, float *__restrict__ r32) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
     r32[t] = (float)b[t];
@@ -956,6 +1053,10 @@ struct DiluState {
   // wavefront sweeps
   unsigned long long *xe = nullptr, *xj = nullptr;
   float4 *lf = nullptr, *ub = nullptr, *ys = nullptr;  // tile-skewed group streams
+  float4 *rs = nullptr;      // refined mode: the inner iterations' r32 in the stream layout
+  double *rz_part = nullptr; // refined mode: per-tile rho partials of the fused backward
+  float *qmap_ptr = nullptr; // the q32 vector qmap describes
+  CUtensorMap qmap;          // q32 in 16 x 16 x 4 boxes (fused forward loads)
   float *seam_f = nullptr, *seam_b = nullptr;
   int2 *order = nullptr;
   WaveCtl *ctl = nullptr;
@@ -1008,6 +1109,10 @@ static int wave_setup(Solver *s) {
       (st = s->alloc((void **)&D->seam_b, sizeof(float) * (size_t)g.ntm2 * g.NRP)) ||
       (st = s->alloc((void **)&D->ctl, sizeof(WaveCtl))))
     return st;
+  if (s->precision == POT3D_FP32_REFINED &&
+      ((st = s->alloc((void **)&D->rs, sizeof(float4) * ng)) ||
+       (st = s->alloc((void **)&D->rz_part, sizeof(double) * D->ntiles))))
+    return st;
   if ((st = encode_padded_map(g, D->r32, false, WE, WJT, WG, &D->rmap))) return st;
   if ((st = encode_padded_map(g, D->z32, false, WE, WJT, 1, &D->zmap, true))) return st;
   // Tickets in order of the tile's first wavefront step WE te + WJT tj
@@ -1032,12 +1137,19 @@ static int wave_setup(Solver *s) {
   D->wave_smem_b = sizeof(WaveSmemB) + 128;
   CK(cudaFuncSetAttribute(k_dilu_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_f));
   CK(cudaFuncSetAttribute(k_dilu_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D->wave_smem_b));
-  int dev = 0, nsm = 0, occ_f = 0, occ_b = 0;
+  CK(cudaFuncSetAttribute(k_dilu_wave<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)D->wave_smem_f));
+  CK(cudaFuncSetAttribute(k_dilu_wave<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)D->wave_smem_b));
+  int dev = 0, nsm = 0, occ_f = 0, occ_b = 0, occ_ff = 0, occ_fb = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_dilu_wave<true>, WAVE_BLOCK, D->wave_smem_f));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_dilu_wave<false>, WAVE_BLOCK, D->wave_smem_b));
-  D->wave_blocks = std::max(1, std::min(std::max(1, std::min(occ_f, occ_b)) * nsm, D->ntiles));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ff, k_dilu_wave<true, true>, WAVE_BLOCK, D->wave_smem_f));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_fb, k_dilu_wave<false, true>, WAVE_BLOCK, D->wave_smem_b));
+  const int occ = std::min(std::min(occ_f, occ_b), std::min(occ_ff, occ_fb));
+  D->wave_blocks = std::max(1, std::min(std::max(1, occ) * nsm, D->ntiles));
   return POT3D_OK;
 }
 
@@ -1253,21 +1365,90 @@ int dilu_sweeps(Solver *s, bool check_status) {
   return pot3d_cuda_status(cudaGetLastError(), "ILU(0) sweeps");
 }
 
+// The residual stream of the fused sweeps from the padded r32 (after the
+// refined solve has formed r32 from an FP64 residual).
+int dilu_r_stream(Solver *s) {
+  DiluState *D = s->dilu;
+  if (!D->rs) {
+    pot3d_set_error("fused ILU(0) sweeps need a solver in the refined mode");
+    return POT3D_ERR_ARG;
+  }
+  k_wave_r_stream<<<grid1d((long long)D->ntiles * (D->nsteps / WG) * WAVE_THREADS), NTHR, 0, s->stream>>>(
+      s->g, D->r32, D->nte, D->ntiles, D->nsteps, D->rs);
+  return pot3d_cuda_status(cudaGetLastError(), "k_wave_r_stream");
+}
+
+// Arguments of the fused sweeps (and the q32 box map, encoded on the host
+// only, so also valid while a stream is being captured).
+static int fused_args(Solver *s, bool check, const float *q32, WaveArgs *out) {
+  DiluState *D = s->dilu;
+  if (!D->rs) {
+    pot3d_set_error("fused ILU(0) sweeps need a solver in the refined mode");
+    return POT3D_ERR_ARG;
+  }
+  if (D->qmap_ptr != q32) {
+    int st;
+    if ((st = encode_padded_map(s->g, q32, false, WE, WJT, WG, &D->qmap))) return st;
+    D->qmap_ptr = const_cast<float *>(q32);
+  }
+  WaveArgs a = wave_args(s, check);
+  a.rs = D->rs;
+  a.rz_part = D->rz_part;
+  *out = a;
+  return POT3D_OK;
+}
+static void launch_wave_fused(Solver *s, bool fwd, const WaveArgs &a) {
+  DiluState *D = s->dilu;
+  if (fwd)
+    k_dilu_wave<true, true><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_f, s->stream>>>(D->qmap, a);
+  else
+    k_dilu_wave<false, true><<<D->wave_blocks, WAVE_BLOCK, D->wave_smem_b, s->stream>>>(D->zmap, a);
+}
+
+// The sweeps of one FP32-inner iteration of the refined mode: the forward
+// applies the inner update's residual half (r32 -= alpha q32, on the
+// residual stream) before its recurrence; the backward computes rho =
+// y.D^-1 y, and its last block ends the iteration (rho, beta, ncg,
+// ernorm).
+int dilu_sweeps_fused(Solver *s, const float *q32) {
+  WaveArgs a;
+  int st;
+  if ((st = fused_args(s, true, q32, &a))) return st;
+  launch_wave_fused(s, true, a);
+  launch_wave_fused(s, false, a);
+  return pot3d_cuda_status(cudaGetLastError(), "fused ILU(0) sweeps");
+}
+
 // Average device time of the forward and of the backward sweep over `reps`
-// applications to the FP32 right-hand side.
+// applications, in the forms the solver iterates with: the plain sweeps on
+// the FP32 right-hand side, or, for a solver in the refined mode, the fused
+// sweeps (its residual stream from the right-hand side, q32 zero, the
+// solve state left alone).
 int dilu_time(Solver *s, int reps, double ms[2]) {
   DiluState *D = s->dilu;
   int st;
   if ((st = dilu_reset(s))) return st;
   k_narrow_rhs<<<grid1d(s->g.Np), NTHR, 0, s->stream>>>(s->g.Np, s->d_b, D->r32);
+  const bool fused = D->rs != nullptr;
+  WaveArgs fa{};
+  if (fused) {
+    if ((st = dilu_r_stream(s)) || (st = fused_args(s, false, s->m_q32, &fa))) return st;
+    CK(cudaMemsetAsync(s->m_q32, 0, sizeof(float) * s->g.Np, s->stream));
+  }
   cudaEvent_t e[3];
   for (auto &x : e) CK(cudaEventCreate(&x));
   ms[0] = ms[1] = 0.0;
   for (int it = 0; it < reps; it++) {
     CK(cudaEventRecord(e[0], s->stream));
-    launch_wave(s, true, false);
-    CK(cudaEventRecord(e[1], s->stream));
-    launch_wave(s, false, false);
+    if (fused) {
+      launch_wave_fused(s, true, fa);
+      CK(cudaEventRecord(e[1], s->stream));
+      launch_wave_fused(s, false, fa);
+    } else {
+      launch_wave(s, true, false);
+      CK(cudaEventRecord(e[1], s->stream));
+      launch_wave(s, false, false);
+    }
     CK(cudaEventRecord(e[2], s->stream));
     CK(cudaEventSynchronize(e[2]));
     float a = 0.f, b = 0.f;

@@ -176,6 +176,7 @@ struct StencilArgs {
   double *s1p;              // PCG: [2][NRP] ring sums of p (parity buffers)
   SolveState *st;
   double *partials;
+  int xslot1;               // refined ILU(0): 1 + the slot of st->xa that receives alpha (0: none)
 };
 
 // Shared-memory layout of the TMA-staged stencil.  Each pipeline stage holds
@@ -267,13 +268,21 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
   int par = 0;
   if (MODE != MODE_AX) {
     const volatile SolveState *vs = a.st;
-    if (vs->status != ST_RUNNING) return;  // uniform: converged or failed
+    if (vs->status != ST_RUNNING) {  // uniform: converged or failed
+      // no iteration: the paired x update applies nothing for it
+      if (a.xslot1 && bx == 0 && by == 0 && bz == 0 && threadIdx.x == 0) a.st->xa[a.xslot1 - 1] = 0.0;
+      return;
+    }
     beta = vs->beta;
     par = vs->par;
   }
   double *kfac = reinterpret_cast<double *>(dyn + L::kfac_off);  // [tk][3]
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~uintptr_t(127));
-  T *pn_ring = reinterpret_cast<T *>(base + S_STAGES * L::bytes);  // [PN_SLOTS][BOX_Y][BOX64_X]
+  // p_new ring [PN_SLOTS][BOX_Y][BOX64_X], FP64 in every mode: the FP32 modes
+  // store each rounded p_new widened once, so the stencil reads it without
+  // a conversion per neighbour (conversions issue at a fraction of the FP64
+  // rate)
+  double *pn_ring = reinterpret_cast<double *>(base + S_STAGES * L::bytes);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -383,23 +392,23 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
     const uint32_t parity = (local / S_STAGES) & 1;
     if (!mbar_wait(&bar[s], parity, WAIT_LIMIT)) abort_flag = 1;
     const unsigned char *st = base + s * L::bytes;
-    T *slot = pn_ring + (local % PN_SLOTS) * (BOX_Y * BOX64_X);
+    double *slot = pn_ring + (local % PN_SLOTS) * (BOX_Y * BOX64_X);
     // own pair
     {
       const int col = 2 + el;
-      slot[(w + 1) * BOX64_X + col] = pnew_at(st, w + 1, col);
-      slot[(w + 1) * BOX64_X + col + 1] = pnew_at(st, w + 1, col + 1);
+      slot[(w + 1) * BOX64_X + col] = (double)pnew_at(st, w + 1, col);
+      slot[(w + 1) * BOX64_X + col + 1] = (double)pnew_at(st, w + 1, col + 1);
     }
     {  // halo: theta rows 0 and TJ+1 (128 points) and radial columns (16)
       if (tid < 2 * TI) {
         const int row = (tid < TI) ? 0 : TJ + 1;
         const int col = 2 + (tid & (TI - 1));
-        slot[row * BOX64_X + col] = pnew_at(st, row, col);
+        slot[row * BOX64_X + col] = (double)pnew_at(st, row, col);
       } else if (tid < 2 * TI + 2 * TJ) {
         const int q = tid - 2 * TI;
         const int row = 1 + (q >> 1);
         const int col = (q & 1) ? TI + 2 : 1;
-        slot[row * BOX64_X + col] = pnew_at(st, row, col);
+        slot[row * BOX64_X + col] = (double)pnew_at(st, row, col);
       }
     }
     __syncthreads();
@@ -410,19 +419,18 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
     }
     if (local >= 2 && v0) {
       const int kk = p_first + local - 1;  // plane whose stencil is now complete
-      const T *sc = pn_ring + ((local - 1) % PN_SLOTS) * (BOX_Y * BOX64_X);
-      const T *sm = pn_ring + ((local - 2) % PN_SLOTS) * (BOX_Y * BOX64_X);
-      const T *sp = slot;
+      const double *sc = pn_ring + ((local - 1) % PN_SLOTS) * (BOX_Y * BOX64_X);
+      const double *sm = pn_ring + ((local - 2) % PN_SLOTS) * (BOX_Y * BOX64_X);
+      const double *sp = slot;
       const int kq = kk - k0;
       const double dpim = kfac[3 * kq], dpip = kfac[3 * kq + 1], dphk = kfac[3 * kq + 2];
       const int col = 2 + el;
-      const T *rowc = sc + (w + 1) * BOX64_X;
-      const T2 xcT = *reinterpret_cast<const T2 *>(rowc + col);
-      const double2 xc = widen2(xcT);
-      const double2 xm = widen2(*reinterpret_cast<const T2 *>(sm + (w + 1) * BOX64_X + col));
-      const double2 xn = widen2(*reinterpret_cast<const T2 *>(sp + (w + 1) * BOX64_X + col));
-      const double2 xjm2 = widen2(*reinterpret_cast<const T2 *>(sc + w * BOX64_X + col));
-      const double2 xjp2 = widen2(*reinterpret_cast<const T2 *>(sc + (w + 2) * BOX64_X + col));
+      const double *rowc = sc + (w + 1) * BOX64_X;
+      const double2 xc = *reinterpret_cast<const double2 *>(rowc + col);
+      const double2 xm = *reinterpret_cast<const double2 *>(sm + (w + 1) * BOX64_X + col);
+      const double2 xn = *reinterpret_cast<const double2 *>(sp + (w + 1) * BOX64_X + col);
+      const double2 xjm2 = *reinterpret_cast<const double2 *>(sc + w * BOX64_X + col);
+      const double2 xjp2 = *reinterpret_cast<const double2 *>(sc + (w + 2) * BOX64_X + col);
       const double xim = (e0 == 0) ? xc.x : (double)rowc[col - 1];
       const double xip = (e0 == g.nrm2 - 1) ? pm * xc.x : xc.y;
       const double xjm = (jj == 0) ? 0.0 : xjm2.x;
@@ -440,12 +448,13 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
         *reinterpret_cast<double2 *>(a.y + id) = make_double2(y, y1);
       } else if constexpr (F32) {
         // q is stored rounded; p.q uses the stored values, as the update does
+        // (the ring holds the rounded p_new exactly, so narrowing it is exact)
         const float2 qv = make_float2((float)y, (float)y1);
-        const float2 own = make_float2(xcT.x, v1 ? xcT.y : 0.0f);
+        const float2 own = make_float2((float)xc.x, v1 ? (float)xc.y : 0.0f);
         *reinterpret_cast<float2 *>(a.q32 + id) = qv;
         *reinterpret_cast<float2 *>(a.p_new32 + id) = own;
-        dot = fma((double)own.x, (double)qv.x, dot);
-        dot = fma((double)own.y, (double)qv.y, dot);
+        dot = fma(xc.x, (double)qv.x, dot);
+        dot = fma(v1 ? xc.y : 0.0, (double)qv.y, dot);
       } else {
         double2 yv = make_double2(y, y1);
         double2 own = make_double2(xc.x, v1 ? xc.y : 0.0);
@@ -481,6 +490,7 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
         } else {
           s->alpha = s->rho / total;
         }
+        if (a.xslot1) s->xa[a.xslot1 - 1] = s->alpha;
       }
     }
   }
@@ -520,8 +530,8 @@ struct UpdateArgs {
 // UPD_ZDOT: r.z with z from the ILU(0) sweeps, ncg+1 and ernorm, no update.
 // UPD_RU: r.z of a freshly computed FP64 residual (a reliable update of the
 // FP32-inner solve): rho and beta are replaced, ncg does not advance, and
-// the status is decided on this residual whatever the recurrence said.
-enum { UPD_ITER = 0, UPD_INIT = 1, UPD_BDOTB = 2, UPD_ZDOT = 3, UPD_RU = 4 };
+// the status is decided on this residual whatever the recurrence said
+// (rz_epilogue).
 
 // R32: the residual (and, for UPD_ITER, p and q) are FP32 vectors; the
 // arithmetic is FP64 and the new residual is rounded once when stored.
@@ -601,28 +611,7 @@ __device__ __forceinline__ void update_body(const Geo &g, const DevMesh &m, cons
       if (KIND == UPD_BDOTB) {
         s->bdotb = total;
       } else {
-        const double rho_it = s->rho;  // UPD_RU: the recurrence's value it replaces
-        if (KIND != UPD_RU) s->rho_old = s->rho;
-        s->rho = total;
-        if (KIND == UPD_ITER || KIND == UPD_ZDOT) s->ncg = s->ncg + 1;
-        // ernorm
-        const double epssq = total / s->bdotb;
-        const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
-        s->epsn = epsn;
-        if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
-        if (KIND == UPD_RU) s->status = ST_RUNNING;
-        if (epsn < s->epscg) {
-          s->status = ST_CONVERGED;
-        } else if (s->ncg >= s->ncgmax) {
-          s->status = ST_MAXIT;
-        } else if (!isfinite(epsn)) {
-          s->status = ST_BREAKDOWN;
-        }
-        if (KIND == UPD_RU) s->rho_true = total;
-        // a reliable update that finds the recurrence far off (its r.z more
-        // than 10x the recurrence's) restarts the direction: p = z
-        const bool restart = KIND == UPD_RU && (!(s->rho_old > 0.0) || total > 10.0 * rho_it);
-        s->beta = (KIND == UPD_INIT || restart) ? 0.0 : total / s->rho_old;
+        rz_epilogue<KIND == UPD_BDOTB ? UPD_ITER : KIND>(s, total);
       }
     }
   }
@@ -676,9 +665,11 @@ __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__r
 // only ever accepted on that FP64 residual.
 // ============================================================================
 
-// ILU(0) inner update: x += alpha p (FP64 x, FP32 p), r32 = r32 - alpha q
-// rounded once; the sweeps then read r32 directly.  Four unknowns per thread
-// (the padded vector length is a multiple of 16).
+// ILU(0) inner update of a batched case: x += alpha p (FP64 x, FP32 p),
+// r32 = r32 - alpha q rounded once; the sweeps then read r32 directly.  Four
+// unknowns per thread (the padded vector length is a multiple of 16).  A
+// single solve runs the solution half for two iterations at once
+// (k_update_x_pair) and the residual half inside its forward sweep.
 __device__ __forceinline__ void update_x32_body(const Geo &g, const UpdateArgs &a, long long t0, long long stride) {
   const volatile SolveState *vs = a.st;
   if (vs->status != ST_RUNNING) return;
@@ -704,8 +695,59 @@ __device__ __forceinline__ void update_x32_body(const Geo &g, const UpdateArgs &
     *reinterpret_cast<float4 *>(a.r32 + id) = rv;
   }
 }
-__global__ void __launch_bounds__(NTHR) k_update_x32(Geo g, UpdateArgs a) {
-  update_x32_body(g, a, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+
+// Solution half of a single refined ILU(0) solve's inner updates, applied
+// to two iterations at once (the residual half runs inside the forward
+// sweep, which reads the residual): x += alpha_a p_a, then x += alpha_b p_b,
+// with p_a, p_b the search directions of two consecutive iterations, which
+// the ping-pong buffers still hold, and the alphas their stencils recorded
+// in st->xa (0 for an iteration that did not run).  The operations are
+// update_x32_body's, in iteration order, so x is bit-identical to updating
+// it every iteration, and the solution vector is read and written once per
+// two iterations.  Four unknowns per thread and pass.
+__global__ void __launch_bounds__(NTHR) k_update_x_pair(Geo g, const SolveState *st, double *__restrict__ x,
+                                                        const float *__restrict__ pa, const float *__restrict__ pb) {
+  const double a0 = *(const volatile double *)&st->xa[0], a1 = *(const volatile double *)&st->xa[1];
+  if (a0 == 0.0 && a1 == 0.0) return;
+  const long long n4 = g.Np / 4;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long id = 4 * t;
+    double2 x0 = *reinterpret_cast<const double2 *>(x + id);
+    double2 x1 = *reinterpret_cast<const double2 *>(x + id + 2);
+    const float4 u = __ldg(reinterpret_cast<const float4 *>(pa + id));
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(pb + id));
+    if (a0 != 0.0) {
+      x0.x = fma(a0, (double)u.x, x0.x);
+      x0.y = fma(a0, (double)u.y, x0.y);
+      x1.x = fma(a0, (double)u.z, x1.x);
+      x1.y = fma(a0, (double)u.w, x1.y);
+    }
+    if (a1 != 0.0) {
+      x0.x = fma(a1, (double)v.x, x0.x);
+      x0.y = fma(a1, (double)v.y, x0.y);
+      x1.x = fma(a1, (double)v.z, x1.x);
+      x1.y = fma(a1, (double)v.w, x1.y);
+    }
+    *reinterpret_cast<double2 *>(x + id) = x0;
+    *reinterpret_cast<double2 *>(x + id + 2) = x1;
+  }
+}
+
+// South-ring partial sums of z for the next stencil after the fused sweeps
+// (which leave no r.z kernel to form them): s1z_part[c][e] = sum over the
+// planes of k chunk c of z(e, ntm1, k)*dph(k)*pl_i, in update_body's order.
+__global__ void k_south_ring_z(Geo g, DevMesh m, const float *__restrict__ z32, double *__restrict__ s1z_part) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int bz = blockIdx.y;
+  if (e >= g.nrm2) return;
+  const int k0 = bz * g.tk_u, k1 = min(k0 + g.tk_u, g.npm2);
+  double s1 = 0.0;
+  for (int kk = k0; kk < k1; kk++) {
+    const double zx = z32[g.idx(e, g.ntm2 - 1, kk)];
+    s1 += __dmul_rn(zx, m.dph[kk + 2]) * m.pl_i;
+  }
+  s1z_part[(long long)bz * g.NRP + e] = s1;
 }
 
 // r = b - q (the FP64 true residual of a reliable update, q = A x) and its
@@ -1091,6 +1133,7 @@ Solver::~Solver() {
   if (evm1) cudaEventDestroy(evm1);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+
   for (void *p : allocs) cudaFree(p);
   if (h_state) cudaFreeHost(h_state);
   if (stream) cudaStreamDestroy(stream);
@@ -1181,6 +1224,12 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
   }
   CK(cudaEventCreate(&ev0));
   CK(cudaEventCreate(&ev1));
+  {
+    int dev = 0, nsm = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    xblocks = (int)std::min<long long>((g.Np / 4 + NTHR - 1) / NTHR, 8LL * nsm);
+  }
   int st = POT3D_OK;
   std::vector<double> r2(nr - 1), dr_i(nr - 1), sth_i(nt), dt_i(nt - 1), dp_i(np);
   for (int i = 0; i < nr - 1; i++) {  // set_local_mesh_r, src/pot3d.F90:2752-2756
@@ -1635,12 +1684,13 @@ namespace pot3d {
 
 float *Solver::r32_inner() { return ifprec == 2 ? dilu_r32(this) : m_r32; }
 
-// One FP32-inner iteration.  Diagonal preconditioner: the PCG32 stencil
-// (p = beta p + a_i r, q = A p, p.q -> alpha) and the update (x += alpha p,
-// r -= alpha q, r.(a_i r) -> rho, beta, epsn).  ILU(0): the PCGZ32 stencil
-// (p = z + beta p), the x/r32 update, the two wavefront sweeps r32 -> z32,
-// and r.z -> rho, beta, epsn.
-int Solver::launch_iteration32() {
+// One FP32-inner iteration at position u of a captured graph.  Diagonal
+// preconditioner: the PCG32 stencil (p = beta p + a_i r, q = A p, p.q ->
+// alpha) and the update (x += alpha p, r -= alpha q, r.(a_i r) -> rho,
+// beta, epsn).  ILU(0): the PCGZ32 stencil (p = z + beta p), at odd u the
+// solution update of this and the previous iteration, the fused sweeps
+// (r32 -= alpha q; r32 -> z32; rho, beta, epsn), the south-ring sums of z.
+int Solver::launch_iteration32(int u) {
   dim3 grid(g.nit, g.njt, g.nkc);
   dim3 gridu(g.nit, g.njt, g.nkc_u);
   StencilArgs sa{};
@@ -1666,13 +1716,15 @@ int Solver::launch_iteration32() {
   if (ifprec == 2) {
     if ((stm = tensor_map(dilu_z32(this), false, &mp.m32[1]))) return stm;
     mp.m32[2] = mp.m32[0];
+    sa.xslot1 = 1 + (u & 1);
     k_stencil<MODE_PCGZ32><<<grid, NTHR, StageLayout<MODE_PCGZ32>::smem, stream>>>(mp, g, m, sa);
-    const long long nb = std::min<long long>((g.Np / 4 + NTHR - 1) / NTHR, 148LL * 8);
-    k_update_x32<<<(int)nb, NTHR, 0, stream>>>(g, ua);
-    int st = dilu_sweeps(this, true);
+    // after every second iteration x += alpha_a p_a + alpha_b p_b (the
+    // previous and this iteration's directions); the sweeps with r32 -=
+    // alpha q, rho, beta and ernorm inside them; the south-ring sums of z
+    if (u & 1) k_update_x_pair<<<xblocks, NTHR, 0, stream>>>(g, d_state, d_x, p32_cur, p32_nxt);
+    int st = dilu_sweeps_fused(this, m_q32);
     if (st) return st;
-    ua.z32 = dilu_z32(this);
-    k_update<UPD_ZDOT, true, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
+    k_south_ring_z<<<dim3((g.nrm2 + 127) / 128, g.nkc_u), 128, 0, stream>>>(g, m, dilu_z32(this), d_s1z);
   } else {
     if ((stm = tensor_map(m_r32, false, &mp.m32[1])) || (stm = tensor_map(d_ai, false, &mp.m32[2]))) return stm;
     k_stencil<MODE_PCG32><<<grid, NTHR, StageLayout<MODE_PCG32>::smem, stream>>>(mp, g, m, sa);
@@ -1688,6 +1740,7 @@ int Solver::reliable_update() {
   int st;
   if ((st = ax_padded(d_x, d_q))) return st;
   k_resid_cast<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_b, d_q, d_r, r32_inner());
+  if (ifprec == 2 && (st = dilu_r_stream(this))) return st;  // the inner iterations' residual
   dim3 gridu(g.nit, g.njt, g.nkc_u);
   UpdateArgs ua{};
   ua.x = d_x;
@@ -1700,7 +1753,7 @@ int Solver::reliable_update() {
     if ((st = dilu_sweeps(this, false))) return st;
     ua.z32 = dilu_z32(this);
     k_update<UPD_RU, true><<<gridu, NTHR, 0, stream>>>(g, m, ua);
-    launches += 4 + sweep_launches();
+    launches += 5 + sweep_launches();
   } else {
     k_update<UPD_RU, false><<<gridu, NTHR, 0, stream>>>(g, m, ua);
     launches += 4;
@@ -1745,6 +1798,8 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   k_cast_r32<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_r, r32_inner());
   launches += 1;
   if (ilu) {
+    if ((st = dilu_r_stream(this))) return st;  // the inner iterations' residual (zero guess)
+    launches += 1;
     if ((st = dilu_reset(this))) return st;
     if ((st = dilu_sweeps(this, false))) return st;
     ua.z32 = dilu_z32(this);
@@ -1774,8 +1829,9 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
     k_resid_cast<<<grid1d(g.Np), NTHR, 0, stream>>>(g.Np, d_b, d_q, d_r, r32_inner());
     launches += 3;
     if (ilu) {
+      if ((st = dilu_r_stream(this))) return st;
       if ((st = dilu_sweeps(this, false))) return st;
-      launches += sweep_launches();
+      launches += 1 + sweep_launches();
     }
   }
   if (ilu)
@@ -1799,7 +1855,7 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     for (int u = 0; u < 2 * U; u++) {  // even count: the p ping-pong returns to m_p32a
-      st = launch_iteration32();
+      st = launch_iteration32(u);
       if (st) {
         cudaStreamEndCapture(stream, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -1813,7 +1869,10 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
     graph32_U = U;
   }
   const long long per_graph = 2LL * U;
-  const long long nodes_per_iter = ilu ? 3 + sweep_launches() : 2;
+  // kernels per iteration (ILU(0): stencil, sweeps, ring sums; plus one
+  // paired x update per two iterations)
+  const long long nodes_per_iter = ilu ? 2 + sweep_launches() : 2;
+  const long long extra_per_graph = ilu ? U : 0;
   double rho_ref = h_state->rho;  // r.z at the last FP64 residual
   int ncg_ref = 0;                // iterations at the last FP64 residual
   int n_refine = 0, stagnant = 0, stalls = 0;
@@ -1821,7 +1880,7 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   while (h_state->status == ST_RUNNING) {
     const int ncg0 = h_state->ncg;
     CK(cudaGraphLaunch(graph32_exec, stream));
-    launches += per_graph * nodes_per_iter;
+    launches += per_graph * nodes_per_iter + extra_per_graph;
     CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     const int status = h_state->status;

@@ -55,6 +55,7 @@ struct Geo {
 struct SolveState {
   double rho, rho_old, alpha, beta, bdotb, epsn, pq, epscg;
   double rho_true;  // refined mode: preconditioned FP64 residual norm^2
+  double xa[2];     // refined ILU(0): alphas of the x updates applied in pairs (0: none)
   int ncg, ncgmax, status, par;
   unsigned int cnt_a, cnt_b, cnt_c, pad0;
   int hist_cap, n_refine, inner, pad1;
@@ -84,6 +85,41 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
     for (int q = 0; q < NT / 32; q++) s += sh[q];
   }
   return s;
+}
+
+// Kinds of the r.z reductions of a PCG solve.  UPD_ITER: the update of an
+// iteration with the diagonal preconditioner; UPD_INIT: the initial
+// residual; UPD_BDOTB: b.M^-1 b; UPD_ZDOT: r.z after the ILU(0) sweeps;
+// UPD_RU: r.z of a fresh FP64 residual (reliable update of the refined mode).
+enum { UPD_ITER = 0, UPD_INIT = 1, UPD_BDOTB = 2, UPD_ZDOT = 3, UPD_RU = 4 };
+
+// What follows a new r.z = total (one thread, KIND != UPD_BDOTB): rho and
+// beta (src/pot3d.F90:4352-4356), ncg and ernorm's epsn and stopping rule
+// (src/pot3d.F90:4430-4483).  UPD_RU replaces the recurrence's rho and
+// decides the status on this residual whatever the recurrence said; a
+// reliable update that finds the recurrence far off (its r.z more than 10x
+// the recurrence's) restarts the direction (beta = 0: p = z).
+template <int KIND>
+__device__ __forceinline__ void rz_epilogue(SolveState *s, double total) {
+  const double rho_it = s->rho;  // UPD_RU: the recurrence's value it replaces
+  if (KIND != UPD_RU) s->rho_old = s->rho;
+  s->rho = total;
+  if (KIND == UPD_ITER || KIND == UPD_ZDOT) s->ncg = s->ncg + 1;
+  const double epssq = total / s->bdotb;
+  const double epsn = (epssq >= 0.0 ? 1.0 : -1.0) * sqrt(fabs(epssq));
+  s->epsn = epsn;
+  if (s->hist && s->ncg < s->hist_cap) s->hist[s->ncg] = epsn;
+  if (KIND == UPD_RU) s->status = ST_RUNNING;
+  if (epsn < s->epscg) {
+    s->status = ST_CONVERGED;
+  } else if (s->ncg >= s->ncgmax) {
+    s->status = ST_MAXIT;
+  } else if (!isfinite(epsn)) {
+    s->status = ST_BREAKDOWN;
+  }
+  if (KIND == UPD_RU) s->rho_true = total;
+  const bool restart = KIND == UPD_RU && (!(s->rho_old > 0.0) || total > 10.0 * rho_it);
+  s->beta = (KIND == UPD_INIT || restart) ? 0.0 : total / s->rho_old;
 }
 
 // Last-block pattern: every block stores its partial at slot b, the block

@@ -45,13 +45,14 @@ struct Solver {
   float *p32_cur = nullptr, *p32_nxt = nullptr;
   cudaGraphExec_t graph32_exec = nullptr;
   int graph32_U = 0;
+  int xblocks = 0;  // grid of the refined ILU(0) iterations' paired solution update
   cudaEvent_t evm0 = nullptr, evm1 = nullptr;
   double refine_ratio = 1e-4;  // reliable update once the recurrence's r.z fell by this factor
   double stall_drop = 0.5;     // an update whose FP64 r.z fell by less than this factor is stagnant
   int stall_limit = 2;         // consecutive stagnant updates that switch the solve to FP64 PCG
   int last_fallback_iters = 0; // FP64 iterations after a switch in the last solve (0: none)
   float *r32_inner();          // the FP32 recurrence residual (the sweeps' input with ILU(0))
-  int launch_iteration32();
+  int launch_iteration32(int u);  // u: position in the captured graph (pairs of iterations)
   int reliable_update();
   int mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, pot3d_solve_info_t *info);
 
@@ -98,6 +99,13 @@ float *dilu_z32(Solver *s);   // FP32 output z = (LU)^-1 r32
 // Forward + backward sweeps r32 -> z32 on s->stream; with check_status the
 // kernels return at once when the PCG state is no longer running.
 int dilu_sweeps(Solver *s, bool check_status);
+// The refined mode's inner iteration: the sweeps fused with the residual
+// half of the update (forward, on the residual stream) and with rho, beta,
+// ncg and ernorm (backward); q32 = A p of the iteration.
+int dilu_sweeps_fused(Solver *s, const float *q32);
+// Refresh the fused sweeps' residual stream from r32 (after r32 was formed
+// from an FP64 residual).
+int dilu_r_stream(Solver *s);
 int encode_padded_map(const Geo &g, const void *ptr, bool fp64, int bx, int by, int bz, CUtensorMap *out,
                       bool interior_only = false);
 int dilu_reset(Solver *s);

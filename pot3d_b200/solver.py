@@ -174,7 +174,8 @@ class Pot3dSolver:
         check(_lib.lib().pot3d_gpu_prec_dev(self._h, C.c_void_p(x.data_ptr())))
 
     def time_sweeps(self, reps: int = 10):
-        """(forward ms, backward ms) of the ILU(0) wavefront sweeps (ifprec=2)."""
+        """(forward ms, backward ms) of the ILU(0) wavefront sweeps (ifprec=2),
+        in the form this solver iterates with (fused in the refined mode)."""
         ms = np.zeros(2)
         check(_lib.lib().pot3d_gpu_time_sweeps(self._h, reps, dptr(ms)))
         return float(ms[0]), float(ms[1])
