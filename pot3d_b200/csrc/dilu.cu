@@ -199,6 +199,7 @@ struct WaveArgs {
   // Fused forms (the FP32-inner iteration of the refined mode):
   float4 *rs;            // forward: the FP32 recurrence residual in the stream layout, read and rewritten
   double *rz_part;       // backward: per-tile partial of rho = y.D^-1 y
+  unsigned *tile_done;   // batched backward: the case's finished tiles in this sweep
 };
 
 __device__ __forceinline__ void wave_publish(unsigned long long *p, unsigned epoch, float v) {
@@ -792,10 +793,14 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2) k_dilu_wave(const __grid_consta
 struct alignas(64) WaveCase {
   CUtensorMap rmap;  // forward: r32 loads
   CUtensorMap zmap;  // backward: z32 stores
+  CUtensorMap qmap;  // fused forward: q32 loads
   WaveArgs a;
 };
 
-template <bool FWD>
+// FUSE: the fused forms of the refined mode's inner iteration (wave_tile);
+// a case's backward tile that finds all the case's other tiles finished
+// ends the case's iteration as k_dilu_wave's last block does.
+template <bool FWD, bool FUSE = false>
 __global__ void __launch_bounds__(WAVE_BLOCK, 2)
     k_dilu_wave_batch(const WaveCase *__restrict__ cases, const int4 *__restrict__ order, int total, WaveCtl *ctl) {
   using Sm = typename WaveSmemSel<FWD>::type;
@@ -843,9 +848,9 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2)
     if (role == 1)
       wave_exchange<FWD>(a, S, f, epoch, a.nsteps / WCH);
     else if (role == 2)
-      wave_copy<FWD>(a, FWD ? &C.rmap : &C.zmap, S, f, gbase, qbase, true);
+      wave_copy<FWD, FUSE>(a, FWD ? (FUSE ? &C.qmap : &C.rmap) : &C.zmap, S, f, gbase, qbase, true);
     else
-      ok = wave_tile<FWD>(a, S, f, epoch, gbase, qbase);
+      ok = wave_tile<FWD, FUSE>(a, S, f, epoch, gbase, qbase);
     if (!ok) S.abort = 1;
     __syncthreads();
     if (S.abort) {
@@ -854,6 +859,26 @@ __global__ void __launch_bounds__(WAVE_BLOCK, 2)
         atomicExch(&a.st->status, ST_TIMEOUT);
       }
       break;
+    }
+    if constexpr (FUSE && !FWD) {
+      // the tile's partial is written (thread 0); the case's last tile ends
+      // the case's iteration
+      __shared__ int case_last;
+      if (threadIdx.x == 0) {
+        __threadfence();
+        case_last = atomicAdd(a.tile_done, 1u) == (unsigned)a.ntiles - 1;
+      }
+      __syncthreads();
+      if (case_last && threadIdx.x < 32) {
+        __threadfence();
+        double t = 0.0;
+        for (int q = threadIdx.x; q < a.ntiles; q += 32) t += __ldcg(a.rz_part + q);
+        t = warp_sum(t);
+        if (threadIdx.x == 0) {
+          if (*(volatile int *)&a.st->status == ST_RUNNING) rz_epilogue<UPD_ZDOT>(a.st, t);
+          *a.tile_done = 0u;
+        }
+      }
     }
     gbase += a.nsteps / WG;
     qbase += FWD ? (a.g.npm2 + WG - 1) / WG : 0;
@@ -1194,7 +1219,9 @@ struct DiluBatch {
   WaveCase *d_cases = nullptr;
   int4 *d_order = nullptr;
   WaveCtl *ctl = nullptr;
-  int total = 0, blocks = 0;
+  unsigned *tile_done = nullptr;  // fused: per case, its backward tiles finished in this sweep
+  int n = 0, total = 0, blocks = 0;
+  bool fused = false;             // every case in the refined mode: the fused sweeps
   size_t smem_f = 0, smem_b = 0;
 };
 
@@ -1203,14 +1230,25 @@ void dilu_batch_destroy(DiluBatch *B) {
   if (B->d_cases) cudaFree(B->d_cases);
   if (B->d_order) cudaFree(B->d_order);
   if (B->ctl) cudaFree(B->ctl);
+  if (B->tile_done) cudaFree(B->tile_done);
   delete B;
 }
+
+static int fused_args(Solver *s, bool check, const float *q32, WaveArgs *out);
 
 int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch **out) {
   *out = nullptr;
   DiluBatch *B = new DiluBatch();
   std::vector<WaveCase> h(n);
   std::vector<int4> ord;
+  B->n = n;
+  B->fused = true;
+  for (int q = 0; q < n; q++) B->fused = B->fused && cases[q]->dilu && cases[q]->dilu->rs;
+  if (B->fused &&
+      pot3d_cuda_status(cudaMalloc(&B->tile_done, sizeof(unsigned) * n), "cudaMalloc(batch tile counters)")) {
+    dilu_batch_destroy(B);
+    return POT3D_ERR_CUDA;
+  }
   for (int q = 0; q < n; q++) {
     DiluState *D = cases[q]->dilu;
     if (!D) {
@@ -1220,7 +1258,17 @@ int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch
     }
     h[q].rmap = D->rmap;
     h[q].zmap = D->zmap;
-    h[q].a = wave_args(cases[q], true);
+    if (B->fused) {
+      int st;
+      if ((st = fused_args(cases[q], true, cases[q]->m_q32, &h[q].a))) {
+        dilu_batch_destroy(B);
+        return st;
+      }
+      h[q].qmap = D->qmap;
+      h[q].a.tile_done = B->tile_done + q;
+    } else {
+      h[q].a = wave_args(cases[q], true);
+    }
     for (int tj = 0; tj < D->ntj; tj++)
       for (int te = 0; te < D->nte; te++) ord.push_back(make_int4(q, te, tj, 0));
   }
@@ -1243,6 +1291,9 @@ int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch
   // Sweep tags of the batch live above 2^31, the cases' own sweeps below it,
   // so the shared exchange buffers never hold a word a later sweep accepts.
   const WaveCtl c0{0u, 0u, 0x80000001u, 0};
+  if (B->fused &&
+      (st = pot3d_cuda_status(cudaMemsetAsync(B->tile_done, 0, sizeof(unsigned) * n, stream), "batch tile counters")))
+    return fail(st);
   if ((st = pot3d_cuda_status(
            cudaMemcpyAsync(B->d_cases, h.data(), sizeof(WaveCase) * n, cudaMemcpyHostToDevice, stream),
            "cudaMemcpy(batch sweep cases)")) ||
@@ -1260,6 +1311,12 @@ int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch
                                                    (int)B->smem_f),
                               "cudaFuncSetAttribute")) ||
       (st = pot3d_cuda_status(cudaFuncSetAttribute(k_dilu_wave_batch<false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_b),
+                              "cudaFuncSetAttribute")) ||
+      (st = pot3d_cuda_status(cudaFuncSetAttribute(k_dilu_wave_batch<true, true>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_f),
+                              "cudaFuncSetAttribute")) ||
+      (st = pot3d_cuda_status(cudaFuncSetAttribute(k_dilu_wave_batch<false, true>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_b),
                               "cudaFuncSetAttribute")) ||
       (st = pot3d_cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) ||
@@ -1285,9 +1342,27 @@ int dilu_batch_sweeps(DiluBatch *B, cudaStream_t stream) {
   return pot3d_cuda_status(cudaGetLastError(), "batched ILU(0) sweeps");
 }
 
-// Clear the batch sweeps' ticket counter and advance their tag.
+// The fused sweeps of the refined mode's inner iteration for every running
+// case (dilu_sweeps_fused per case, with the cases' q32 in their tables).
+int dilu_batch_sweeps_fused(DiluBatch *B, cudaStream_t stream) {
+  if (!B->fused) {
+    pot3d_set_error("fused batched ILU(0) sweeps need every case in the refined mode");
+    return POT3D_ERR_ARG;
+  }
+  k_dilu_wave_batch<true, true><<<B->blocks, WAVE_BLOCK, B->smem_f, stream>>>(B->d_cases, B->d_order, B->total,
+                                                                                    B->ctl);
+  k_dilu_wave_batch<false, true><<<B->blocks, WAVE_BLOCK, B->smem_b, stream>>>(B->d_cases, B->d_order,
+                                                                                     B->total, B->ctl);
+  return pot3d_cuda_status(cudaGetLastError(), "fused batched ILU(0) sweeps");
+}
+bool dilu_batch_fused(const DiluBatch *B) { return B && B->fused; }
+
+// Clear the batch sweeps' ticket counter (and the fused backward's per-case
+// tile counters, which a sweep that gave up can leave behind) and advance
+// their tag.
 int dilu_batch_reset(DiluBatch *B, cudaStream_t stream) {
   k_wave_reset<<<1, 1, 0, stream>>>(B->ctl);
+  if (B->fused) CK(cudaMemsetAsync(B->tile_done, 0, sizeof(unsigned) * B->n, stream));
   return pot3d_cuda_status(cudaGetLastError(), "k_wave_reset(batch)");
 }
 

@@ -359,8 +359,13 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
   const double pm = m.pm_r1;
   double dot = 0.0;
 
-  // p_new at (row, col) of the stage tile; col counts FP64 columns.  The
-  // FP32 modes form it in FP64 and round it once.
+  // p_new at (row, col) of the stage tile; col counts FP64 columns.  PCG32
+  // forms it in FP64 and rounds it once; PCGZ32 forms it with one FP32 fma
+  // (beta rounded to FP32 once per block): every operand is already FP32 and
+  // the result is stored in FP32, and the two conversions per operand and
+  // the rounding of an FP64 fma would load the conversion pipe, which bounds
+  // this kernel's issue, for a difference at the last bit of the FP32 value.
+  const float beta32 = (float)beta;
   auto pnew_at = [&](const unsigned char *st, int row, int col) -> T {
     const double *t0 = reinterpret_cast<const double *>(st);
     if constexpr (MODE == MODE_PCG32) {
@@ -373,7 +378,7 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
       const float *f0 = reinterpret_cast<const float *>(st);
       const float *f1 = reinterpret_cast<const float *>(st + TILE32_PITCH);
       const int c = row * BOX32_X + col + 2;
-      return (float)fma(beta, (double)f0[c], (double)f1[c]);
+      return __fmaf_rn(beta32, f0[c], f1[c]);
     } else if (MODE == MODE_AX) {
       return t0[row * BOX64_X + col];
     } else if (MODE == MODE_PCG) {
@@ -386,6 +391,7 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
     }
   };
 
+  T2 own_cur{}, own_prev{};
   int local = 0;
   for (; local < n_planes; local++) {
     const int s = local % S_STAGES;
@@ -393,11 +399,15 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
     if (!mbar_wait(&bar[s], parity, WAIT_LIMIT)) abort_flag = 1;
     const unsigned char *st = base + s * L::bytes;
     double *slot = pn_ring + (local % PN_SLOTS) * (BOX_Y * BOX64_X);
-    // own pair
+    // own pair (kept in registers in storage precision for the output of
+    // this plane, which follows one plane later)
+    own_prev = own_cur;
     {
       const int col = 2 + el;
-      slot[(w + 1) * BOX64_X + col] = (double)pnew_at(st, w + 1, col);
-      slot[(w + 1) * BOX64_X + col + 1] = (double)pnew_at(st, w + 1, col + 1);
+      own_cur.x = pnew_at(st, w + 1, col);
+      own_cur.y = pnew_at(st, w + 1, col + 1);
+      slot[(w + 1) * BOX64_X + col] = (double)own_cur.x;
+      slot[(w + 1) * BOX64_X + col + 1] = (double)own_cur.y;
     }
     {  // halo: theta rows 0 and TJ+1 (128 points) and radial columns (16)
       if (tid < 2 * TI) {
@@ -448,9 +458,10 @@ __device__ __forceinline__ void stencil_body(const StencilMaps &maps, const Geo 
         *reinterpret_cast<double2 *>(a.y + id) = make_double2(y, y1);
       } else if constexpr (F32) {
         // q is stored rounded; p.q uses the stored values, as the update does
-        // (the ring holds the rounded p_new exactly, so narrowing it is exact)
+        // (own_prev is the stored p_new of this plane; the ring holds it
+        // exactly, so xc equals it)
         const float2 qv = make_float2((float)y, (float)y1);
-        const float2 own = make_float2((float)xc.x, v1 ? (float)xc.y : 0.0f);
+        const float2 own = make_float2(own_prev.x, v1 ? own_prev.y : 0.0f);
         *reinterpret_cast<float2 *>(a.q32 + id) = qv;
         *reinterpret_cast<float2 *>(a.p_new32 + id) = own;
         dot = fma(xc.x, (double)qv.x, dot);
@@ -705,13 +716,13 @@ __device__ __forceinline__ void update_x32_body(const Geo &g, const UpdateArgs &
 // update_x32_body's, in iteration order, so x is bit-identical to updating
 // it every iteration, and the solution vector is read and written once per
 // two iterations.  Four unknowns per thread and pass.
-__global__ void __launch_bounds__(NTHR) k_update_x_pair(Geo g, const SolveState *st, double *__restrict__ x,
-                                                        const float *__restrict__ pa, const float *__restrict__ pb) {
+__device__ __forceinline__ void x_pair_body(const Geo &g, const SolveState *st, double *__restrict__ x,
+                                            const float *__restrict__ pa, const float *__restrict__ pb, long long t0,
+                                            long long stride) {
   const double a0 = *(const volatile double *)&st->xa[0], a1 = *(const volatile double *)&st->xa[1];
   if (a0 == 0.0 && a1 == 0.0) return;
   const long long n4 = g.Np / 4;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = t0; t < n4; t += stride) {
     const long long id = 4 * t;
     double2 x0 = *reinterpret_cast<const double2 *>(x + id);
     double2 x1 = *reinterpret_cast<const double2 *>(x + id + 2);
@@ -733,13 +744,16 @@ __global__ void __launch_bounds__(NTHR) k_update_x_pair(Geo g, const SolveState 
     *reinterpret_cast<double2 *>(x + id + 2) = x1;
   }
 }
+__global__ void __launch_bounds__(NTHR) k_update_x_pair(Geo g, const SolveState *st, double *__restrict__ x,
+                                                        const float *__restrict__ pa, const float *__restrict__ pb) {
+  x_pair_body(g, st, x, pa, pb, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
 
 // South-ring partial sums of z for the next stencil after the fused sweeps
 // (which leave no r.z kernel to form them): s1z_part[c][e] = sum over the
 // planes of k chunk c of z(e, ntm1, k)*dph(k)*pl_i, in update_body's order.
-__global__ void k_south_ring_z(Geo g, DevMesh m, const float *__restrict__ z32, double *__restrict__ s1z_part) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int bz = blockIdx.y;
+__device__ __forceinline__ void south_ring_z_body(const Geo &g, const DevMesh &m, const float *__restrict__ z32,
+                                                  double *__restrict__ s1z_part, int e, int bz) {
   if (e >= g.nrm2) return;
   const int k0 = bz * g.tk_u, k1 = min(k0 + g.tk_u, g.npm2);
   double s1 = 0.0;
@@ -748,6 +762,9 @@ __global__ void k_south_ring_z(Geo g, DevMesh m, const float *__restrict__ z32, 
     s1 += __dmul_rn(zx, m.dph[kk + 2]) * m.pl_i;
   }
   s1z_part[(long long)bz * g.NRP + e] = s1;
+}
+__global__ void k_south_ring_z(Geo g, DevMesh m, const float *__restrict__ z32, double *__restrict__ s1z_part) {
+  south_ring_z_body(g, m, z32, s1z_part, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
 // r = b - q (the FP64 true residual of a reliable update, q = A x) and its
@@ -2034,12 +2051,23 @@ __global__ void __launch_bounds__(NTHR) k_update_r32_batch(const BatchInst *__re
   const unsigned local = blockIdx.x - I.off_r;
   update_r32_body(I.g, I.ua[par], (long long)local * NTHR + threadIdx.x, (long long)I.nb_r * NTHR);
 }
-// FP32-inner ILU(0): x += alpha p (FP64 x), r32 -= alpha q, every running case.
-__global__ void __launch_bounds__(NTHR) k_update_x32_batch(const BatchInst *__restrict__ in, int n, int par) {
+// FP32-inner ILU(0), every running case: the paired solution update after
+// an odd graph position (the directions of parity 0 and 1, k_update_x_pair),
+// and the south-ring sums of z after the fused sweeps (k_south_ring_z).
+__global__ void __launch_bounds__(NTHR) k_update_x_pair_batch(const BatchInst *__restrict__ in, int n) {
   const int i = batch_find(in, n, blockIdx.x, BATCH_R32);
   const BatchInst &I = in[i];
   const unsigned local = blockIdx.x - I.off_r;
-  update_x32_body(I.g, I.ua[par], (long long)local * NTHR + threadIdx.x, (long long)I.nb_r * NTHR);
+  x_pair_body(I.g, I.ua[1].st, I.ua[1].x, I.ua[0].p32, I.ua[1].p32, (long long)local * NTHR + threadIdx.x,
+              (long long)I.nb_r * NTHR);
+}
+__global__ void __launch_bounds__(NTHR) k_south_ring_z_batch(const BatchInst *__restrict__ in, int n) {
+  const int i = batch_find(in, n, blockIdx.x, BATCH_R32);
+  const BatchInst &I = in[i];
+  const unsigned local = blockIdx.x - I.off_r;
+  const int neb = (I.g.nrm2 + NTHR - 1) / NTHR;
+  for (int w = (int)local; w < neb * I.g.nkc_u; w += (int)I.nb_r)
+    south_ring_z_body(I.g, I.m, I.ua[0].z32, I.ua[0].s1z_part, (w % neb) * NTHR + threadIdx.x, w / neb);
 }
 
 struct Batch {
@@ -2151,6 +2179,7 @@ static int batch_table(Batch &B) {
       if (B.precision == POT3D_FP32_REFINED) {  // the operands of launch_iteration32
         float *o32 = par == 0 ? s.m_p32a : s.m_p32b, *n32 = par == 0 ? s.m_p32b : s.m_p32a;
         sa.p_new32 = n32;
+        if (ilu) sa.xslot1 = 1 + par;  // the paired x update (k_update_x_pair_batch)
         sa.q32 = s.m_q32;
         ua.p32 = n32;
         ua.q32 = s.m_q32;
@@ -2240,7 +2269,8 @@ static int batch_init(Batch &B, int ncgmax, double epscg) {
       CK(cudaMemsetAsync(s.m_p32a, 0, sizeof(float) * s.g.Np, B.stream));
       k_cast_r32<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_r, s.r32_inner());
       if (B.ifprec == 2) {
-        if ((st = dilu_reset(&s)) || (st = dilu_sweeps(&s, false))) return st;
+        // the fused sweeps' residual stream (zero guess: r = b)
+        if ((st = dilu_r_stream(&s)) || (st = dilu_reset(&s)) || (st = dilu_sweeps(&s, false))) return st;
         ua.z32 = dilu_z32(&s);
         k_update<UPD_BDOTB, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
       } else {
@@ -2249,7 +2279,7 @@ static int batch_init(Batch &B, int ncgmax, double epscg) {
       if (guessed) {
         if ((st = s.ax_padded(s.d_x, s.d_q))) return st;
         k_resid_cast<<<grid1d(s.g.Np), NTHR, 0, B.stream>>>(s.g.Np, s.d_b, s.d_q, s.d_r, s.r32_inner());
-        if (B.ifprec == 2 && (st = dilu_sweeps(&s, false))) return st;
+        if (B.ifprec == 2 && ((st = dilu_r_stream(&s)) || (st = dilu_sweeps(&s, false)))) return st;
       }
       if (B.ifprec == 2)
         k_update<UPD_INIT, true><<<gridu, NTHR, 0, B.stream>>>(s.g, s.m, ua);
@@ -2293,9 +2323,9 @@ static void batch_iteration(Batch &B, int par) {
   if (B.precision == POT3D_FP32_REFINED) {  // launch_iteration32's sequence, every running case per launch
     if (B.ifprec == 2) {
       k_stencil_batch<MODE_PCGZ32><<<B.nblk_s, NTHR, StageLayout<MODE_PCGZ32>::smem, B.stream>>>(B.d_tab, n, par);
-      k_update_x32_batch<<<B.nblk_r, NTHR, 0, B.stream>>>(B.d_tab, n, par);
-      dilu_batch_sweeps(B.wave, B.stream);
-      k_update_batch<UPD_ZDOT, true, true><<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
+      if (par == 1) k_update_x_pair_batch<<<B.nblk_r, NTHR, 0, B.stream>>>(B.d_tab, n);
+      dilu_batch_sweeps_fused(B.wave, B.stream);
+      k_south_ring_z_batch<<<B.nblk_r, NTHR, 0, B.stream>>>(B.d_tab, n);
     } else {
       k_stencil_batch<MODE_PCG32><<<B.nblk_s, NTHR, StageLayout<MODE_PCG32>::smem, B.stream>>>(B.d_tab, n, par);
       k_update_batch<UPD_ITER, false, true><<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
@@ -2312,7 +2342,14 @@ static void batch_iteration(Batch &B, int par) {
     k_update_batch<UPD_ITER, false><<<B.nblk_u, NTHR, 0, B.stream>>>(B.d_tab, n, par);
   }
 }
-static int batch_launches_per_iteration(const Batch &B) { return B.ifprec == 2 ? 5 : 2; }
+// Kernels per batched iteration (the refined ILU(0) form adds one paired x
+// update per two iterations, batch_extra_launches_per_graph).
+static int batch_launches_per_iteration(const Batch &B) {
+  return B.ifprec == 2 ? (B.precision == POT3D_FP32_REFINED ? 4 : 5) : 2;
+}
+static int batch_extra_launches_per_graph(const Batch &B) {
+  return B.ifprec == 2 && B.precision == POT3D_FP32_REFINED ? B.U : 0;
+}
 
 // Capture 2U batched iterations of the current table into B.graph.
 static int batch_capture(Batch &B) {
@@ -2643,7 +2680,7 @@ extern "C" int pot3d_gpu_batch_solve(pot3d_gpu_batch *h, int ncgmax, double epsc
     }
     for (int q : run) B.ncg0[q] = B.pin[q].ncg;
     CK(cudaGraphLaunch(B.graph, B.stream));
-    launches += 2LL * B.U * batch_launches_per_iteration(B);
+    launches += 2LL * B.U * batch_launches_per_iteration(B) + batch_extra_launches_per_graph(B);
     if ((st = batch_poll(B))) return st;
     after_graph = true;
   }

@@ -121,6 +121,8 @@ int dilu_sweep_launches(Solver *s);
 struct DiluBatch;
 int dilu_batch_setup(Solver *const *cases, int n, cudaStream_t stream, DiluBatch **out);
 int dilu_batch_sweeps(DiluBatch *b, cudaStream_t stream);
+int dilu_batch_sweeps_fused(DiluBatch *b, cudaStream_t stream);  // refined mode (dilu_sweeps_fused per case)
+bool dilu_batch_fused(const DiluBatch *b);
 int dilu_batch_reset(DiluBatch *b, cudaStream_t stream);
 void dilu_batch_destroy(DiluBatch *b);
 
