@@ -198,7 +198,7 @@ struct WaveArgs {
   int pad;               // nsteps - (npm2 + WSK): idle steps, trailing forward, leading backward
   // Fused forms (the FP32-inner iteration of the refined mode):
   float4 *rs;            // forward: the FP32 recurrence residual in the stream layout, read and rewritten
-  double *rz_part;       // backward: per-tile partial of rho = y.D^-1 y
+  double *rz_part;       // backward: per-tile partial of rho = r.z
   unsigned *tile_done;   // batched backward: the case's finished tiles in this sweep
 };
 
@@ -518,12 +518,16 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
   // streamed r32 of the step (the operations of the unfused update, so the
   // values are the same) at the start of each step group, off the steps'
   // dependent chain, and written back to the stream.  Fused backward:
-  // rho = y.D^-1 y, which equals r.M^-1 r for M = L (D + U) with L = I +
-  // E D^-1 and U = E^T (the D-ILU factors of the symmetric A), accumulated
-  // in FP64 from the y and dinv the sweep reads anyway.
+  // rho = r.z of the stored r32 and the z32 it computes, accumulated in FP64
+  // (the r.z update's sum in another order); the thread reads its r32 from
+  // the residual stream, which is in the forward's step order like the y
+  // stream, one group ahead of use with a plain coalesced load (its latency
+  // off the steps' chain, no shared memory).
   double alpha = 0.0;
   if constexpr (FUSE && FWD) alpha = *(const volatile double *)&a.st->alpha;
   double rz = 0.0;
+  float4 r_cur = make_float4(0.f, 0.f, 0.f, 0.f), r_next = r_cur;
+  if constexpr (FUSE && !FWD) r_next = a.rs[((size_t)ti * G + (G - 1)) * WAVE_THREADS + T];
   // forward: plane p = t - sk of this line sits in slot (qbase + p / WG) % WPG,
   // row p % WG (p < 0 at the first steps: the entry is never read)
   int p_sub = 0, p_slot = 0;
@@ -585,6 +589,10 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         c2 = S.ub[sl][2][T];
         c3 = S.ub[sl][3][T];
         yin4 = S.yin[sl][T];
+      }
+      if constexpr (FUSE && !FWD) {  // this group's residuals; the next group's load is issued
+        r_cur = r_next;
+        if (gi + 1 < G) r_next = a.rs[((size_t)ti * G + (G - 2 - gi)) * WAVE_THREADS + T];
       }
       float y4[WG], rn4[WG], vin4[WG];
       if constexpr (FWD && FUSE) {
@@ -656,9 +664,10 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
           seam_y = (act && kk == npm2 - 1) ? y : seam_y;
           if (act) S.zout[kk % WROUT][T] = y;
           if constexpr (FUSE) {
-            // y and dinv are exact zeros where the thread has no point
-            const double yv = (double)v_in;
-            rz = fma(yv * (double)k3, yv, rz);
+            // the point's r32 (forward step nsteps-1-t, component 3-u, as
+            // for y); r and z are exact zeros where the thread has no point
+            const float rr = u == 0 ? r_cur.w : u == 1 ? r_cur.z : u == 2 ? r_cur.y : r_cur.x;
+            rz = fma((double)rr, (double)y, rz);
           }
         }
         S.y[t & 1][jl][el] = y;
@@ -1482,9 +1491,9 @@ static void launch_wave_fused(Solver *s, bool fwd, const WaveArgs &a) {
 
 // The sweeps of one FP32-inner iteration of the refined mode: the forward
 // applies the inner update's residual half (r32 -= alpha q32, on the
-// residual stream) before its recurrence; the backward computes rho =
-// y.D^-1 y, and its last block ends the iteration (rho, beta, ncg,
-// ernorm).
+// residual stream) before its recurrence; the backward computes rho = r.z
+// (r32 from the residual stream), and its last block ends the iteration
+// (rho, beta, ncg, ernorm).
 int dilu_sweeps_fused(Solver *s, const float *q32) {
   WaveArgs a;
   int st;
