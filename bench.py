@@ -58,13 +58,13 @@ METRIC = "solve s to 1e-9 resid: learned+FP32-refined vs plain FP64 PCG on 1 B20
 # The ILU(0) application moves 12 B forward (r32, d, y) and 12 B backward
 # (y, d, z32).  In the refined mode's inner iteration the forward sweep also
 # applies the residual half of the update (q32 read, r32 written: +8 B; its
-# r32 read is the sweep's own) and the backward sweep forms rho from the y
-# and d it reads (no bytes).
+# r32 read is the sweep's own) and the backward sweep forms rho = r.z (r32
+# read: +4 B; z is its own output).
 BYTES_PER_UNKNOWN_ITER = {("fp64", 1): 80.0, ("fp64", 2): 104.0, ("fp32_refined", 1): 40.0,
                           ("fp32_refined", 2): 64.0}
 BYTES_PER_REFINE = 24.0
 SWEEP_BYTES_PER_UNKNOWN = {"k_dilu_wave<fwd>": 12.0, "k_dilu_wave<bwd>": 12.0,
-                           "k_dilu_wave<fwd,fused>": 20.0, "k_dilu_wave<bwd,fused>": 12.0}
+                           "k_dilu_wave<fwd,fused>": 20.0, "k_dilu_wave<bwd,fused>": 16.0}
 
 
 def sweep_names(precision: str):

@@ -1860,11 +1860,13 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
 
-  // Graphs of 2U iterations, at most 16: a reliable update is only made
-  // between graphs, and it must come before the recurrence has drifted far
-  // from the FP64 residual (small grids converge many decades per graph).
+  // Graphs of 2U iterations (about 2 ms, at most 16): a reliable update is
+  // only made between graphs, and it must come before the recurrence has
+  // drifted far from the FP64 residual (small grids converge many decades
+  // per graph); the host's poll between graphs leaves the GPU idle for a
+  // few microseconds.
   const double est_iter_s = (ilu ? 100.0 : 60.0) * (double)g.Np / 5.0e12 + 6e-6;
-  int U = (int)std::ceil(0.5e-3 / est_iter_s);
+  int U = (int)std::ceil(2.0e-3 / est_iter_s);
   U = std::max(1, std::min(U, 8));
   if (!graph32_exec || graph32_U != U) {
     if (graph32_exec) cudaGraphExecDestroy(graph32_exec);
