@@ -748,6 +748,39 @@ __global__ void __launch_bounds__(NTHR) k_update_x_pair(Geo g, const SolveState 
                                                         const float *__restrict__ pa, const float *__restrict__ pb) {
   x_pair_body(g, st, x, pa, pb, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
+// The single solve's form: four iterations at once, x += a_0 p_0 + a_1 p_1 +
+// a_2 p_2 + a_3 p_3 in iteration order (the directions of four consecutive
+// iterations, in the four rotating buffers), 8 B per unknown and iteration.
+__global__ void __launch_bounds__(NTHR) k_update_x_quad(Geo g, const SolveState *st, double *__restrict__ x,
+                                                        const float *__restrict__ p0, const float *__restrict__ p1,
+                                                        const float *__restrict__ p2, const float *__restrict__ p3) {
+  double a[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) a[i] = *(const volatile double *)&st->xa[i];
+  if (a[0] == 0.0 && a[1] == 0.0 && a[2] == 0.0 && a[3] == 0.0) return;
+  const float *p[4] = {p0, p1, p2, p3};
+  const long long n4 = g.Np / 4;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long id = 4 * t;
+    double2 x0 = *reinterpret_cast<const double2 *>(x + id);
+    double2 x1 = *reinterpret_cast<const double2 *>(x + id + 2);
+    float4 v[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) v[i] = __ldg(reinterpret_cast<const float4 *>(p[i] + id));
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      if (a[i] != 0.0) {
+        x0.x = fma(a[i], (double)v[i].x, x0.x);
+        x0.y = fma(a[i], (double)v[i].y, x0.y);
+        x1.x = fma(a[i], (double)v[i].z, x1.x);
+        x1.y = fma(a[i], (double)v[i].w, x1.y);
+      }
+    }
+    *reinterpret_cast<double2 *>(x + id) = x0;
+    *reinterpret_cast<double2 *>(x + id + 2) = x1;
+  }
+}
 
 // South-ring partial sums of z for the next stencil after the fused sweeps
 // (which leave no r.z kernel to form them): s1z_part[c][e] = sum over the
@@ -1319,6 +1352,11 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
     const size_t fb = sizeof(float) * (size_t)g.Np;
     if ((st = alloc((void **)&m_p32a, fb)) || (st = alloc((void **)&m_p32b, fb)) || (st = alloc((void **)&m_q32, fb)))
       return st;
+    if (ifprec == 2) {
+      m_p32q[0] = m_p32a;
+      m_p32q[1] = m_p32b;
+      if ((st = alloc((void **)&m_p32q[2], fb)) || (st = alloc((void **)&m_p32q[3], fb))) return st;
+    }
     if (ifprec != 2 && (st = alloc((void **)&m_r32, fb))) return st;  // ILU(0) uses the sweeps' r32
     CK(cudaEventCreate(&evm0));
     CK(cudaEventCreate(&evm1));
@@ -1704,12 +1742,17 @@ float *Solver::r32_inner() { return ifprec == 2 ? dilu_r32(this) : m_r32; }
 // One FP32-inner iteration at position u of a captured graph.  Diagonal
 // preconditioner: the PCG32 stencil (p = beta p + a_i r, q = A p, p.q ->
 // alpha) and the update (x += alpha p, r -= alpha q, r.(a_i r) -> rho,
-// beta, epsn).  ILU(0): the PCGZ32 stencil (p = z + beta p), at odd u the
-// solution update of this and the previous iteration, the fused sweeps
-// (r32 -= alpha q; r32 -> z32; rho, beta, epsn), the south-ring sums of z.
+// beta, epsn).  ILU(0): the PCGZ32 stencil (p = z + beta p), at every
+// fourth u the solution update of the last four iterations, the fused
+// sweeps (r32 -= alpha q; r32 -> z32; rho, beta, epsn), the south-ring sums
+// of z.
 int Solver::launch_iteration32(int u) {
   dim3 grid(g.nit, g.njt, g.nkc);
   dim3 gridu(g.nit, g.njt, g.nkc_u);
+  if (ifprec == 2) {  // the rotation of four directions: position u reads buffer u % 4, writes the next
+    p32_cur = m_p32q[u & 3];
+    p32_nxt = m_p32q[(u + 1) & 3];
+  }
   StencilArgs sa{};
   sa.p_new32 = p32_nxt;
   sa.q32 = m_q32;
@@ -1733,12 +1776,13 @@ int Solver::launch_iteration32(int u) {
   if (ifprec == 2) {
     if ((stm = tensor_map(dilu_z32(this), false, &mp.m32[1]))) return stm;
     mp.m32[2] = mp.m32[0];
-    sa.xslot1 = 1 + (u & 1);
+    sa.xslot1 = 1 + (u & 3);
     k_stencil<MODE_PCGZ32><<<grid, NTHR, StageLayout<MODE_PCGZ32>::smem, stream>>>(mp, g, m, sa);
-    // after every second iteration x += alpha_a p_a + alpha_b p_b (the
-    // previous and this iteration's directions); the sweeps with r32 -=
-    // alpha q, rho, beta and ernorm inside them; the south-ring sums of z
-    if (u & 1) k_update_x_pair<<<xblocks, NTHR, 0, stream>>>(g, d_state, d_x, p32_cur, p32_nxt);
+    // after every fourth iteration x += the four iterations' alpha p (their
+    // directions are buffers 1, 2, 3, 0); the sweeps with r32 -= alpha q,
+    // rho, beta and ernorm inside them; the south-ring sums of z
+    if ((u & 3) == 3)
+      k_update_x_quad<<<xblocks, NTHR, 0, stream>>>(g, d_state, d_x, m_p32q[1], m_p32q[2], m_p32q[3], m_p32q[0]);
     int st = dilu_sweeps_fused(this, m_q32);
     if (st) return st;
     k_south_ring_z<<<dim3((g.nrm2 + 127) / 128, g.nkc_u), 128, 0, stream>>>(g, m, dilu_z32(this), d_s1z);
@@ -1800,7 +1844,7 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   last_fallback_iters = 0;
   p32_cur = m_p32a;
   p32_nxt = m_p32b;
-  CK(cudaMemsetAsync(p32_cur, 0, sizeof(float) * g.Np, stream));
+  CK(cudaMemsetAsync(p32_cur, 0, sizeof(float) * g.Np, stream));  // (m_p32q[0] with ILU(0))
   CK(cudaMemsetAsync(d_s1p, 0, sizeof(double) * 2 * g.NRP, stream));
   CK(cudaMemcpyAsync(d_r, d_b, sizeof(double) * g.Np, cudaMemcpyDeviceToDevice, stream));
   UpdateArgs ua{};
@@ -1868,12 +1912,13 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   const double est_iter_s = (ilu ? 100.0 : 60.0) * (double)g.Np / 5.0e12 + 6e-6;
   int U = (int)std::ceil(2.0e-3 / est_iter_s);
   U = std::max(1, std::min(U, 8));
+  if (ilu) U = (U + 1) & ~1;  // whole groups of four iterations (the rotation and the x update)
   if (!graph32_exec || graph32_U != U) {
     if (graph32_exec) cudaGraphExecDestroy(graph32_exec);
     graph32_exec = nullptr;
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    for (int u = 0; u < 2 * U; u++) {  // even count: the p ping-pong returns to m_p32a
+    for (int u = 0; u < 2 * U; u++) {  // even count (ILU(0): multiple of 4): the directions return to m_p32a
       st = launch_iteration32(u);
       if (st) {
         cudaStreamEndCapture(stream, &graph);
@@ -1888,10 +1933,10 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
     graph32_U = U;
   }
   const long long per_graph = 2LL * U;
-  // kernels per iteration (ILU(0): stencil, sweeps, ring sums; plus one
-  // paired x update per two iterations)
+  // kernels per iteration (ILU(0): stencil, sweeps, ring sums; plus one x
+  // update per four iterations)
   const long long nodes_per_iter = ilu ? 2 + sweep_launches() : 2;
-  const long long extra_per_graph = ilu ? U : 0;
+  const long long extra_per_graph = ilu ? U / 2 : 0;
   double rho_ref = h_state->rho;  // r.z at the last FP64 residual
   int ncg_ref = 0;                // iterations at the last FP64 residual
   int n_refine = 0, stagnant = 0, stalls = 0;
@@ -1924,7 +1969,11 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
     CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     if (h_state->status != ST_RUNNING) break;
-    if (ran & 1) {
+    if (ilu && (ran & 3)) {
+      // the graph stopped inside a group of four: the newest p is in buffer
+      // ran % 4, the next graph's first iteration reads buffer 0
+      CK(cudaMemcpyAsync(m_p32q[0], m_p32q[ran & 3], sizeof(float) * g.Np, cudaMemcpyDeviceToDevice, stream));
+    } else if (!ilu && (ran & 1)) {
       // the graph stopped after an odd number of iterations: the newest p is
       // in the buffer the next graph writes first
       CK(cudaMemcpyAsync(p32_cur, p32_nxt, sizeof(float) * g.Np, cudaMemcpyDeviceToDevice, stream));

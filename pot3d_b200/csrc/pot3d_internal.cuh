@@ -55,7 +55,7 @@ struct Geo {
 struct SolveState {
   double rho, rho_old, alpha, beta, bdotb, epsn, pq, epscg;
   double rho_true;  // refined mode: preconditioned FP64 residual norm^2
-  double xa[2];     // refined ILU(0): alphas of the x updates applied in pairs (0: none)
+  double xa[4];     // refined ILU(0): alphas of the x updates applied in groups (0: none)
   int ncg, ncgmax, status, par;
   unsigned int cnt_a, cnt_b, cnt_c, pad0;
   int hist_cap, n_refine, inner, pad1;

@@ -42,10 +42,13 @@ struct Solver {
 
   // FP32-inner / FP64-refined mode (both preconditioners)
   float *m_p32a = nullptr, *m_p32b = nullptr, *m_r32 = nullptr, *m_q32 = nullptr;
+  // ILU(0): four directions in rotation (a, b and two more), so the solution
+  // update is applied once per four iterations
+  float *m_p32q[4] = {nullptr, nullptr, nullptr, nullptr};
   float *p32_cur = nullptr, *p32_nxt = nullptr;
   cudaGraphExec_t graph32_exec = nullptr;
   int graph32_U = 0;
-  int xblocks = 0;  // grid of the refined ILU(0) iterations' paired solution update
+  int xblocks = 0;  // grid of the refined ILU(0) iterations' grouped solution update
   cudaEvent_t evm0 = nullptr, evm1 = nullptr;
   double refine_ratio = 1e-4;  // reliable update once the recurrence's r.z fell by this factor
   double stall_drop = 0.5;     // an update whose FP64 r.z fell by less than this factor is stagnant
