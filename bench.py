@@ -4,8 +4,9 @@ One step = one complete solve of the PFSS workload 255x361x721 (65.3 M
 unknowns, seeded synthetic Br: spherical harmonics l<=40 plus 20 bipoles)
 to the reference's stopping rule epsn < epscg = 1e-9 (ernorm,
 src/pot3d.F90:4430-4433), by the headline method: the learned initial
-guess (the FNO trained for this grid, its inference inside the timed
-region) followed by FP32-inner / FP64-refined PCG with the reference's
+guess (the FNO trained on 2000 solves at 127x181x361, run on this grid's
+theta-phi points with its radial levels interpolated onto this mesh, its
+inference inside the timed region) followed by FP32-inner / FP64-refined PCG with the reference's
 ILU(0) preconditioner (ifprec=2).  Timed in the same run, on the same
 inputs: the plain FP64 PCG with the diagonal preconditioner (ifprec=1, the
 reference's default) and FP64 PCG with ILU(0) from zero (same
@@ -383,8 +384,9 @@ def main():
                     help="oracle PCG iterations of the reference arm's sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warm-start", default="auto",
-                    help="FNO weights (.npz) for the learned initial guess; 'auto' uses "
-                         "pot3d_b200/weights/fno_<workload>.npz when present; 'off' solves from zero")
+                    help="FNO weights (.npz) for the learned initial guess, run on the workload's grid; "
+                         "'auto' uses pot3d_b200/weights/fno_<workload>.npz when present, else the operator "
+                         "trained at 127x181x361; 'off' solves from zero")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the FP64 solves timed beside the headline solve")
     ap.add_argument("--no-parity", action="store_true", help="skip the 1e-11 parity solves")
@@ -428,17 +430,23 @@ def main():
     rt = torch.empty(N, dtype=torch.float64, device="cuda")
     bt = torch.tensor(b, device="cuda")
 
-    # Learned initial guess (FNO trained on this grid), inference timed as part of the solve.
+    # Learned initial guess, inference timed as part of the solve: the FNO
+    # trained for this grid when there is one, else the operator trained at
+    # 127x181x361 run on this grid (resolution-free in theta-phi, its radial
+    # levels interpolated onto this mesh's).  Trained on PFSS maps, it also
+    # starts the open-field workload closer than zero (fewer iterations to
+    # the same tolerance), though far from its solution.
     wpath = args.warm_start
     if wpath == "auto":
         cand = os.path.join(ROOT, "pot3d_b200", "weights", f"fno_{args.workload}.npz")
-        wpath = cand if os.path.exists(cand) else "off"
+        base = os.path.join(ROOT, "pot3d_b200", "weights", "fno_pfss_127x181x361.npz")
+        wpath = cand if os.path.exists(cand) else base
     model = None
     if wpath != "off":
-        from pot3d_b200.fno import FNO, grid_from_mesh
+        from pot3d_b200.fno import FNO
         from pot3d_b200.tc import LAUNCHES, check_errors
         from pot3d_b200.warmstart import Inputs
-        model = FNO.load(wpath, grid_from_mesh(mesh))
+        model = FNO.load_resampled(wpath, mesh)
         inputs = Inputs(model)
         v, sig = inputs.normalized(br0)
         br0n_h = torch.from_numpy(v).view(1, -1).pin_memory()
@@ -629,7 +637,10 @@ def main():
         "gpu_launches": int(np.sum([q["launches"] for q in steps])), "true_residual": steps[-1]["true_resid"],
         "epsn": steps[-1]["epsn"], "inference_s": steps[-1]["inference_s"],
         "plain_fp64": plain, "fp64_same_preconditioner": same_prec, "parity": parity,
-        "warm_start": None if model is None else {"weights": os.path.relpath(wpath, ROOT), "zero_guess": zero_guess},
+        "warm_start": None if model is None else {
+            "weights": os.path.relpath(wpath, ROOT),
+            "trained_interior_theta_phi_r": "x".join(str(int(v)) for v in np.load(wpath)["grid"][:3]),
+            "radial_levels_resampled": getattr(model, "R_out", None) is not None, "zero_guess": zero_guess},
         "throughput_solves_per_s": ws / t_dev,
     }
     print(json.dumps(line), flush=True)

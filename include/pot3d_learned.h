@@ -52,6 +52,14 @@ int pot3d_fno_inputs(const float *br0n, const float *consts, long long B, long l
  * sigma FP64 on the device, x FP64 in the solver's packed layout). */
 int pot3d_fno_guess(const float *out, long long B, long long npos, int Rp, int R, const double *sigma, double *x,
                     void *stream);
+/* The same for a network trained on another radial mesh: its Rs output
+ * levels (Rs <= Rp) are interpolated linearly onto the solver's R levels,
+ * x[b][pos*R + i] = sigma[b] * (o[idx[i]] + w[i] * (o[idx[i]+1] - o[idx[i]]))
+ * with o = out[b][pos] and 0 <= idx[i] <= Rs-2 (idx, w: device arrays of R;
+ * w outside [0, 1] extrapolates at the ends).  No counterpart in the
+ * reference, whose initial guess is zero (src/pot3d.F90:3924). */
+int pot3d_fno_guess_resampled(const float *out, long long B, long long npos, int Rp, int Rs, const int *idx,
+                              const double *w, int R, const double *sigma, double *x, void *stream);
 
 #ifdef __cplusplus
 }

@@ -290,7 +290,37 @@ __global__ void k_guess(const float *__restrict__ out, long long B, long long np
     x[t] = (double)out[bp * Rp + i] * sigma[b];
   }
 }
+// The same with the radial levels resampled: the network's Rs levels (those
+// of the mesh it was trained on) interpolated linearly onto the solver's R
+// levels, level i from source levels idx[i] and idx[i]+1 with weight w[i]
+// (outside [0, 1] at the ends: linear extrapolation).
+__global__ void k_guess_resampled(const float *__restrict__ out, long long B, long long npos, int Rp,
+                                  const int *__restrict__ idx, const double *__restrict__ w, int R,
+                                  const double *__restrict__ sigma, double *__restrict__ x) {
+  const long long n = B * npos * R;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % R);
+    const long long bp = t / R;  // b * npos + pos
+    const long long b = bp / npos;
+    const float *o = out + bp * Rp + idx[i];
+    const double lo = (double)o[0], hi = (double)o[1];
+    x[t] = fma(w[i], hi - lo, lo) * sigma[b];
+  }
+}
 }  // namespace
+
+extern "C" int pot3d_fno_guess_resampled(const float *out, long long B, long long npos, int Rp, int Rs,
+                                         const int *idx, const double *w, int R, const double *sigma, double *x,
+                                         void *stream) {
+  if (B < 1 || npos < 1 || R < 1 || Rs < 2 || Rp < Rs) {
+    pot3d_set_error("pot3d_fno_guess_resampled: bad sizes");
+    return POT3D_ERR_ARG;
+  }
+  k_guess_resampled<<<grid_for(B * npos * R), 256, 0, (cudaStream_t)stream>>>(out, B, npos, Rp, idx, w, R, sigma,
+                                                                              x);
+  return pot3d_cuda_status(cudaGetLastError(), "pot3d_fno_guess_resampled");
+}
 
 extern "C" int pot3d_fno_guess(const float *out, long long B, long long npos, int Rp, int R, const double *sigma,
                                double *x, void *stream) {

@@ -56,6 +56,7 @@ def _L():
         L.pot3d_fno_adam.argtypes = [vp, vp, vp, vp, vp, ll, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, vp]
         L.pot3d_fno_inputs.argtypes = [vp, vp, ll, ll, vp, vp]
         L.pot3d_fno_guess.argtypes = [vp, ll, ll, C.c_int, C.c_int, vp, vp, vp]
+        L.pot3d_fno_guess_resampled.argtypes = [vp, ll, ll, C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp]
         L._fno_typed = True
     return L
 
@@ -135,6 +136,23 @@ class Grid:
 def grid_from_mesh(mesh) -> Grid:
     return Grid(mesh.nt - 2, mesh.np - 2, mesh.nr - 2, mesh.th[1:-1].copy(), mesh.dth[1:-1].copy(),
                 mesh.ph[1:-1].copy(), mesh.dph[1:-1].copy())
+
+
+def radial_weights(rh_src, rh_dst, r0_dst, r1_dst):
+    """Linear interpolation from the interior half-mesh levels of rh_src
+    (ghosts included; its boundaries sit midway between ghost and first
+    point) onto those of rh_dst (boundaries r0_dst, r1_dst), in the radial
+    coordinate normalised to [0, 1] between the boundaries: level i of the
+    destination is o[idx[i]] + w[i] (o[idx[i]+1] - o[idx[i]]), with w
+    outside [0, 1] extrapolating past the first and last source levels."""
+    rh_src = np.asarray(rh_src, np.float64)
+    r0_src = 0.5 * (rh_src[0] + rh_src[1])
+    r1_src = 0.5 * (rh_src[-2] + rh_src[-1])
+    s_src = (rh_src[1:-1] - r0_src) / (r1_src - r0_src)
+    s_dst = (np.asarray(rh_dst, np.float64)[1:-1] - r0_dst) / (r1_dst - r0_dst)
+    idx = np.clip(np.searchsorted(s_src, s_dst) - 1, 0, len(s_src) - 2).astype(np.int32)
+    w = (s_dst - s_src[idx]) / (s_src[idx + 1] - s_src[idx])
+    return idx, w
 
 
 def bases(g: Grid, mt=16, mp=32):
@@ -372,11 +390,49 @@ class FNO:
     @classmethod
     def load(cls, path, grid: "Grid"):
         """A model saved by save() for the same grid (theta, phi, radial sizes)."""
-        import torch
         z = np.load(path)
-        nth, nph, R, W_, nl, mt, mp, hidden, in_ch = (int(v) for v in z["grid"])
+        nth, nph, R = (int(v) for v in z["grid"][:3])
         if (nth, nph, R) != (grid.nth, grid.nph, grid.R):
             raise ValueError(f"{path}: trained for {nth}x{nph}x{R}, not {grid.nth}x{grid.nph}x{grid.R}")
+        return cls._from_saved(path, z, grid)
+
+    @classmethod
+    def load_resampled(cls, path, mesh):
+        """A model saved by save() applied on the grid of `mesh`, which may
+        differ from the training grid: the theta-phi layers are free of the
+        resolution (quadrature-weighted truncated bases, pointwise lifts and
+        projections), so the network runs on mesh's theta-phi points as it
+        is; its radial levels (the output channels, those of the training
+        mesh) are interpolated linearly onto mesh's in the radial coordinate
+        normalised to [0, 1] between the inner and outer radius.  The
+        training mesh's half-mesh radii are the file's "rh" when it has them,
+        else those of the PFSS law the models here are trained on (r in
+        [1, 2.5], drratio 2.5, nr = R + 2)."""
+        z = np.load(path)
+        Rs = int(z["grid"][2])
+        g = grid_from_mesh(mesh)
+        m = cls._from_saved(path, z, Grid(g.nth, g.nph, Rs, g.th, g.dth, g.ph, g.dph))
+        if Rs != g.R:
+            if "rh" in z:
+                rh_s = np.asarray(z["rh"], np.float64)
+            else:
+                from .host import make_mesh
+                rh_s = make_mesh(Rs + 2, 5, 8).rh
+            m.set_radial(rh_s, mesh.rh, mesh.r[0], mesh.r[-1])
+        return m
+
+    def set_radial(self, rh_src, rh_dst, r0_dst, r1_dst):
+        """Interpolation of the network's radial levels (half-mesh radii
+        rh_src, ghosts included) onto the interior levels of rh_dst."""
+        import torch
+        idx, w = radial_weights(rh_src, rh_dst, r0_dst, r1_dst)
+        self.R_out = len(idx)
+        self.radial = (torch.tensor(idx).cuda(), torch.tensor(w, dtype=torch.float64).cuda())
+
+    @classmethod
+    def _from_saved(cls, path, z, grid: "Grid"):
+        import torch
+        _, _, _, W_, nl, mt, mp, hidden, in_ch = (int(v) for v in z["grid"])
         m = cls(grid, width=W_, layers=nl, mt=mt, mp=mp, hidden=hidden, in_ch=in_ch)
         for k in list(m.p):
             if "bf16_" + k in z:
@@ -391,21 +447,30 @@ class FNO:
 
     def predict(self, x, sigma, out=None):
         """Initial guesses in the packed solver layout, FP64 [B, N] (into
-        `out` when given); sigma: per-sample scales (host or FP64 device)."""
+        `out` when given); sigma: per-sample scales (host or FP64 device).
+        With radial levels resampled (load_resampled) N counts the solver's
+        levels."""
         import torch
         y = self.forward(x)  # FP32 [B, nph, nth, Rp]
         B = x.shape[0]
         g = self.g
         npos = g.nph * g.nth
+        R = getattr(self, "R_out", g.R)
         assert y.dtype == torch.float32 and y.is_contiguous() and y.numel() == B * npos * self.Rp
         sig = sigma if hasattr(sigma, "data_ptr") else torch.tensor(np.asarray(sigma, np.float64), device="cuda")
         assert sig.dtype == torch.float64 and sig.numel() == B
-        guess = out if out is not None else torch.empty((B, npos * g.R), dtype=torch.float64, device="cuda")
-        if guess.dtype != torch.float64 or not guess.is_contiguous() or guess.numel() != B * npos * g.R:
+        guess = out if out is not None else torch.empty((B, npos * R), dtype=torch.float64, device="cuda")
+        if guess.dtype != torch.float64 or not guess.is_contiguous() or guess.numel() != B * npos * R:
             raise ValueError("predict: out must be a contiguous FP64 tensor of B x N")
         _count()
-        _lib.check(_L().pot3d_fno_guess(C.c_void_p(y.data_ptr()), B, npos, self.Rp, g.R, C.c_void_p(sig.data_ptr()),
-                                        C.c_void_p(guess.data_ptr()), _stream()))
+        if getattr(self, "radial", None) is not None:
+            idx, w = self.radial
+            _lib.check(_L().pot3d_fno_guess_resampled(
+                C.c_void_p(y.data_ptr()), B, npos, self.Rp, g.R, C.c_void_p(idx.data_ptr()), C.c_void_p(w.data_ptr()),
+                R, C.c_void_p(sig.data_ptr()), C.c_void_p(guess.data_ptr()), _stream()))
+        else:
+            _lib.check(_L().pot3d_fno_guess(C.c_void_p(y.data_ptr()), B, npos, self.Rp, g.R,
+                                            C.c_void_p(sig.data_ptr()), C.c_void_p(guess.data_ptr()), _stream()))
         return guess
 
 

@@ -22,3 +22,28 @@ def test_recorded_held_out_evaluation():
     assert ev["cases"] == 200 and len(rec["cases"]) == 200
     assert ev["iteration_ratio"] < 1.0 and ev["fewer_iterations_cases"] == 200
     assert ev["sol_rel_diff_max"] < 1e-7
+
+
+def test_radial_resampling_weights():
+    """The operator runs on other grids with its radial levels (the training
+    mesh's) interpolated linearly onto the solver mesh's, in the radius
+    normalised between the boundaries: exact for a field linear in that
+    coordinate, interior levels interpolated, the outermost extrapolated."""
+    import numpy as np
+    from pot3d_b200 import host
+    from pot3d_b200.fno import radial_weights
+    src = host.make_mesh(127, 5, 8)
+    for nr, r1 in ((255, 2.5), (511, 2.5), (63, 2.5), (95, 2.7)):
+        dst = host.make_mesh(nr, 5, 8, r1=r1)
+        idx, w = radial_weights(src.rh, dst.rh, dst.r[0], dst.r[-1])
+        assert len(idx) == nr - 2 and idx.min() >= 0 and idx.max() <= 123
+
+        def lin(m):
+            s = (m.rh[1:-1] - m.r[0]) / (m.r[-1] - m.r[0])
+            return 3.0 * s - 0.25
+        o = lin(src)
+        got = o[idx] + w * (o[idx + 1] - o[idx])
+        assert np.max(np.abs(got - lin(dst))) < 1e-13
+        # only levels beyond the source's outermost ones (at the two ends) extrapolate
+        inner = np.flatnonzero((w >= 0.0) & (w <= 1.0))
+        assert np.all(np.diff(inner) == 1) and inner[0] <= 2 and inner[-1] >= len(w) - 3
