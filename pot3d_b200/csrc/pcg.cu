@@ -676,46 +676,17 @@ __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__r
 // only ever accepted on that FP64 residual.
 // ============================================================================
 
-// ILU(0) inner update of a batched case: x += alpha p (FP64 x, FP32 p),
-// r32 = r32 - alpha q rounded once; the sweeps then read r32 directly.  Four
-// unknowns per thread (the padded vector length is a multiple of 16).  A
-// single solve runs the solution half for two iterations at once
-// (k_update_x_pair) and the residual half inside its forward sweep.
-__device__ __forceinline__ void update_x32_body(const Geo &g, const UpdateArgs &a, long long t0, long long stride) {
-  const volatile SolveState *vs = a.st;
-  if (vs->status != ST_RUNNING) return;
-  const double alpha = vs->alpha;
-  const long long n4 = g.Np / 4;
-  for (long long t = t0; t < n4; t += stride) {
-    const long long id = 4 * t;
-    double2 x0 = *reinterpret_cast<const double2 *>(a.x + id);
-    double2 x1 = *reinterpret_cast<const double2 *>(a.x + id + 2);
-    const float4 pv = __ldg(reinterpret_cast<const float4 *>(a.p32 + id));
-    const float4 qv = __ldg(reinterpret_cast<const float4 *>(a.q32 + id));
-    float4 rv = *reinterpret_cast<const float4 *>(a.r32 + id);
-    x0.x = fma(alpha, (double)pv.x, x0.x);
-    x0.y = fma(alpha, (double)pv.y, x0.y);
-    x1.x = fma(alpha, (double)pv.z, x1.x);
-    x1.y = fma(alpha, (double)pv.w, x1.y);
-    rv.x = (float)fma(-alpha, (double)qv.x, (double)rv.x);
-    rv.y = (float)fma(-alpha, (double)qv.y, (double)rv.y);
-    rv.z = (float)fma(-alpha, (double)qv.z, (double)rv.z);
-    rv.w = (float)fma(-alpha, (double)qv.w, (double)rv.w);
-    *reinterpret_cast<double2 *>(a.x + id) = x0;
-    *reinterpret_cast<double2 *>(a.x + id + 2) = x1;
-    *reinterpret_cast<float4 *>(a.r32 + id) = rv;
-  }
-}
-
-// Solution half of a single refined ILU(0) solve's inner updates, applied
-// to two iterations at once (the residual half runs inside the forward
-// sweep, which reads the residual): x += alpha_a p_a, then x += alpha_b p_b,
-// with p_a, p_b the search directions of two consecutive iterations, which
-// the ping-pong buffers still hold, and the alphas their stencils recorded
-// in st->xa (0 for an iteration that did not run).  The operations are
-// update_x32_body's, in iteration order, so x is bit-identical to updating
-// it every iteration, and the solution vector is read and written once per
-// two iterations.  Four unknowns per thread and pass.
+// Solution half of the refined ILU(0) inner update (the residual half,
+// r32 = r32 - alpha q rounded once, runs inside the forward sweep, which
+// reads the residual), applied to groups of iterations: x += alpha_a p_a,
+// then x += alpha_b p_b, with p_a, p_b the search directions of two
+// consecutive iterations, which the ping-pong buffers still hold, and the
+// alphas their stencils recorded in st->xa (0 for an iteration that did not
+// run).  One fma of FP64 x with the FP32 direction per point and iteration,
+// in iteration order, so x is bit-identical to updating it every iteration,
+// and the solution vector is read and written once per group.  Four
+// unknowns per thread and pass.  Batches use pairs; a single solve groups
+// four (k_update_x_quad).
 __device__ __forceinline__ void x_pair_body(const Geo &g, const SolveState *st, double *__restrict__ x,
                                             const float *__restrict__ pa, const float *__restrict__ pb, long long t0,
                                             long long stride) {
@@ -744,11 +715,7 @@ __device__ __forceinline__ void x_pair_body(const Geo &g, const SolveState *st, 
     *reinterpret_cast<double2 *>(x + id + 2) = x1;
   }
 }
-__global__ void __launch_bounds__(NTHR) k_update_x_pair(Geo g, const SolveState *st, double *__restrict__ x,
-                                                        const float *__restrict__ pa, const float *__restrict__ pb) {
-  x_pair_body(g, st, x, pa, pb, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
-}
-// The single solve's form: four iterations at once, x += a_0 p_0 + a_1 p_1 +
+// The single solve's groups: four iterations at once, x += a_0 p_0 + a_1 p_1 +
 // a_2 p_2 + a_3 p_3 in iteration order (the directions of four consecutive
 // iterations, in the four rotating buffers), 8 B per unknown and iteration.
 __global__ void __launch_bounds__(NTHR) k_update_x_quad(Geo g, const SolveState *st, double *__restrict__ x,
@@ -2103,7 +2070,7 @@ __global__ void __launch_bounds__(NTHR) k_update_r32_batch(const BatchInst *__re
   update_r32_body(I.g, I.ua[par], (long long)local * NTHR + threadIdx.x, (long long)I.nb_r * NTHR);
 }
 // FP32-inner ILU(0), every running case: the paired solution update after
-// an odd graph position (the directions of parity 0 and 1, k_update_x_pair),
+// an odd graph position (the directions of parity 0 and 1, x_pair_body),
 // and the south-ring sums of z after the fused sweeps (k_south_ring_z).
 __global__ void __launch_bounds__(NTHR) k_update_x_pair_batch(const BatchInst *__restrict__ in, int n) {
   const int i = batch_find(in, n, blockIdx.x, BATCH_R32);
