@@ -19,9 +19,10 @@ preconditioner), both to 1e-9.
 value: device time of the solve (CUDA events on the library's stream around
 the PCG initialisation and iterations, plus the guess's inference on
 torch's stream), inputs resident in HBM.
-e2e: the same solve through the C-ABI with page-locked host buffers
-(pot3d_gpu_cgsolve), the map upload, the guess download and the
-host<->device copies of x and r inside the timed wall-clock region.
+e2e: the same solve end to end from page-locked host buffers, wall clock:
+the upload of the map (the guess is inferred from it on the device) and of
+the right-hand side, the solve through the C-ABI (pot3d_gpu_cgsolve_dev),
+and the download of x and r (cgsolve's outputs).
 The working set (about 3 GB of vectors plus 2.5 GB of sweep coefficient
 streams) is 40x the 126 MB L2, so no flush is needed between steps.
 parity: the headline method solved to 1e-11 against FP64 PCG (ILU(0)) to
@@ -493,9 +494,13 @@ def main():
     x_timed = xt.cpu().numpy()
     fallback = s.refine_info()[1] if args.precision == "fp32_refined" else 0
 
-    # End to end through the host-pointer C-ABI (H2D + solve + D2H) on pinned
-    # host buffers; with the learned guess also the map's upload and the
-    # guess's download.
+    # End to end, wall clock, from page-locked host buffers: the inputs (the
+    # right-hand side, and the boundary map the guess is inferred from) go up,
+    # the result (x and the residual r, cgsolve's outputs) comes down.  From
+    # zero: the host-pointer C-ABI (pot3d_gpu_cgsolve: x and r uploaded, x
+    # and r downloaded).  With the learned guess: the map's upload, the
+    # inference into the device x, r's upload, the device-pointer C-ABI
+    # (pot3d_gpu_cgsolve_dev) and the downloads of x and r.
     x_pin = torch.zeros(N, dtype=torch.float64, pin_memory=True)
     r_pin = torch.empty(N, dtype=torch.float64, pin_memory=True)
     x_h, r_h = x_pin.numpy(), r_pin.numpy()
@@ -508,15 +513,19 @@ def main():
         if model is not None:
             br0n_d.copy_(br0n_h)
             guess_into(xt)
+            rt.copy_(r_pin)
+            if s.cgsolve_dev(xt, rt, epscg=args.epscg) != 0:
+                raise SystemExit("e2e solve did not converge")
             x_pin.copy_(xt)
+            r_pin.copy_(rt)
+            torch.cuda.synchronize()
         else:
             x_h[:] = 0.0
-        if s.cgsolve(x_h, r_h, epscg=args.epscg) != 0:
-            raise SystemExit("e2e solve did not converge")
+            if s.cgsolve(x_h, r_h, epscg=args.epscg) != 0:
+                raise SystemExit("e2e solve did not converge")
         e2e.append(time.perf_counter() - t0)
     if model is not None:
-        h2d += 4 * br0n_h.numel()
-        d2h += 8 * N
+        h2d = 8 * N + 4 * br0n_h.numel()
         check_errors()
     t_e2e = reduce_max(float(np.mean(e2e)), ws)
 

@@ -757,6 +757,7 @@ __device__ __forceinline__ void south_ring_z_body(const Geo &g, const DevMesh &m
   if (e >= g.nrm2) return;
   const int k0 = bz * g.tk_u, k1 = min(k0 + g.tk_u, g.npm2);
   double s1 = 0.0;
+#pragma unroll 8  // the loads of a block of planes issue together; the sum keeps its order
   for (int kk = k0; kk < k1; kk++) {
     const double zx = z32[g.idx(e, g.ntm2 - 1, kk)];
     s1 += __dmul_rn(zx, m.dph[kk + 2]) * m.pl_i;
