@@ -226,6 +226,30 @@ def evaluate(model: FNO, inputs: Inputs, mesh, solver, seeds, lmax, nbip, eps=1e
     return summ, rows
 
 
+def evaluate_saved(args, mesh):
+    """The --evaluate record: a saved operator on this grid's held-out seeds."""
+    import torch
+    z = np.load(args.evaluate)
+    model = FNO.load_resampled(args.evaluate, mesh)
+    inputs = Inputs(model)
+    solver = Pot3dSolver(mesh, case_br0(mesh, args.test_seed0, args.lmax, args.nbip), ifprec=args.ifprec,
+                         precision=args.precision)
+    plain = Pot3dSolver(mesh, case_br0(mesh, args.test_seed0, args.lmax, args.nbip), ifprec=1) if args.plain else None
+    t0 = time.time()
+    summ, rows = evaluate(model, inputs, mesh, solver, range(args.test_seed0, args.test_seed0 + args.test),
+                          args.lmax, args.nbip, plain=plain)
+    torch.cuda.synchronize()
+    cfg = {k: v for k, v in vars(args).items() if k in ("nr", "nt", "np", "lmax", "nbip", "test", "test_seed0",
+                                                       "ifprec", "precision", "plain", "evaluate")}
+    cfg["trained_interior_theta_phi_r"] = "x".join(str(int(v)) for v in z["grid"][:3])
+    cfg["radial_levels_resampled"] = getattr(model, "R_out", None) is not None
+    rep = dict(config=cfg, evaluation=dict(seconds=time.time() - t0, **summ), cases=rows)
+    with open(args.out, "w") as fh:
+        json.dump(rep, fh, indent=1)
+    print(json.dumps(summ), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--nr", type=int, default=127)
@@ -247,9 +271,14 @@ def main(argv=None):
     ap.add_argument("--ifprec", type=int, default=2, help="preconditioner of the generating and evaluating solves")
     ap.add_argument("--precision", default="fp32_refined", choices=["fp64", "fp32_refined"])
     ap.add_argument("--plain", action="store_true", help="also time the plain FP64 diagonal PCG from zero")
+    ap.add_argument("--evaluate", default="",
+                    help="only evaluate the saved operator at this path on the held-out seeds of this grid (run on "
+                         "the grid's theta-phi points, its radial levels interpolated when the grids differ)")
     args = ap.parse_args(argv)
     import torch
     mesh = host.make_mesh(args.nr, args.nt, args.np)
+    if args.evaluate:
+        return evaluate_saved(args, mesh)
     solver = Pot3dSolver(mesh, case_br0(mesh, args.train_seed0, args.lmax, args.nbip), ifprec=args.ifprec,
                          precision=args.precision)
     model = FNO(grid_from_mesh(mesh))

@@ -47,3 +47,21 @@ def test_radial_resampling_weights():
         # only levels beyond the source's outermost ones (at the two ends) extrapolate
         inner = np.flatnonzero((w >= 0.0) & (w <= 1.0))
         assert np.all(np.diff(inner) == 1) and inner[0] <= 2 and inner[-1] >= len(w) - 3
+
+
+def test_recorded_evaluation_on_the_headline_grid():
+    """The committed evaluation of the same operator run on the 255x361x721
+    grid (python -m pot3d_b200.warmstart --nr 255 --nt 361 --np 721 --test
+    20 --evaluate ...): 20 held-out seeds, the radial levels resampled, fewer
+    iterations on every seed, guesses within 3% of the solution, and the
+    solutions from either start within 1e-7."""
+    with open(WEIGHTS + "_at_255x361x721.json") as fh:
+        rec = json.load(fh)
+    cfg = rec["config"]
+    assert (cfg["nr"], cfg["nt"], cfg["np"]) == (255, 361, 721)
+    assert cfg["evaluate"].endswith("fno_pfss_127x181x361.npz") and cfg["radial_levels_resampled"]
+    assert cfg["test_seed0"] >= 5000 and cfg["test"] == 20  # outside the training seeds 1000-2999
+    ev = rec["evaluation"]
+    assert ev["cases"] == 20 and len(rec["cases"]) == 20
+    assert ev["fewer_iterations_cases"] == 20 and ev["iteration_ratio"] < 0.9
+    assert ev["guess_rel_err_max"] < 0.03 and ev["sol_rel_diff_max"] < 1e-7
