@@ -72,3 +72,59 @@ def check_errors(device="cuda"):
     e = _err_flag(device)
     if int(e.item()) != 0:
         raise RuntimeError("pot3d_tc_gemm: a bounded wait ran out on the device")
+
+
+# Shapes of the learned operator's GEMMs at 255x361x721 (359 x 719 theta-phi
+# positions) and a square reference shape.
+BENCH_SHAPES = ((258121, 32, 64, "lift and pointwise layers"), (258121, 128, 64, "first projection"),
+                (258121, 128, 128, "radial projection (128 channels)"), (8192, 8192, 8192, "square"))
+
+
+def main(argv=None):
+    """Throughput of tc_gemm (CUDA events, 3 warm-up and 20 timed launches)
+    at the operator's shapes, beside torch.matmul on the same operands; with
+    --one, a single 8192^3 product after warm-up (for a profiler)."""
+    import argparse
+    import json
+
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--one", action="store_true")
+    args = ap.parse_args(argv)
+    if args.one:
+        A = torch.randn(8192, 8192, device="cuda").bfloat16()
+        B = torch.randn(8192, 8192, device="cuda").bfloat16()
+        out = torch.empty(8192, 8192, device="cuda", dtype=torch.float32)
+        for _ in range(3):
+            tc_gemm(A, B, out=out)
+        torch.cuda.synchronize()
+        check_errors()
+        return 0
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for M, N, K, name in BENCH_SHAPES:
+        A = torch.randn(M, K, device="cuda").bfloat16()
+        B = torch.randn(N, K, device="cuda").bfloat16()
+        out = torch.empty(M, N, device="cuda", dtype=torch.float32)
+        ms = timed(lambda: tc_gemm(A, B, out=out))
+        ref = timed(lambda: torch.matmul(A, B.T))
+        check_errors()
+        flops, nbytes = 2.0 * M * N * K, 2.0 * (M * K + N * K) + 4.0 * M * N
+        print(json.dumps(dict(shape=[M, N, K], name=name, ms=ms, tflops=flops / ms / 1e9, gbs=nbytes / ms / 1e6,
+                              torch_ms=ref, torch_tflops=flops / ref / 1e9)), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
