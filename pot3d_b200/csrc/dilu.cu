@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 #include "pot3d_internal.cuh"
@@ -608,84 +609,106 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
           vin4[u] = (float)fma(-alpha, (double)qv, (double)ro);  // r32 - alpha q
         }
       }
+      // The group's steps, in two compiled forms.  INNER: every thread's
+      // plane is strictly inside its line at all four steps (neither the
+      // first nor the last plane of the sweep, where the seam coupling and
+      // the seam value live, and no idle step), so the seam term, its
+      // coefficient select and the per-step activity test drop out; the
+      // remaining terms keep lusol's order (the dropped term subtracted an
+      // exact zero, so values are unchanged up to the sign of an exact-zero
+      // result).  Most groups of a sweep are inner.
+      auto steps = [&](auto inner_tag) -> bool {
+        constexpr bool INNER = decltype(inner_tag)::value;
+        bool aborted = false;
 #pragma unroll
-      for (int u = 0; u < WG; u++) {
-        const int t = gi * WG + u;
-        const int uc = h * WG + u;  // step within the chunk
-        const float *yprev = &S.y[(t + 1) & 1][0][0];  // values of step t-1
-        const float k0 = u == 0 ? c0.x : u == 1 ? c0.y : u == 2 ? c0.z : c0.w;
-        const float k1 = u == 0 ? c1.x : u == 1 ? c1.y : u == 2 ? c1.z : c1.w;
-        const float k2 = u == 0 ? c2.x : u == 1 ? c2.y : u == 2 ? c2.z : c2.w;
-        const float k3 = u == 0 ? c3.x : u == 1 ? c3.y : u == 2 ? c3.z : c3.w;
-        // backward y: forward step nsteps-1-t, component 3-u of the group
-        float v_in = u == 0 ? yin4.w : u == 1 ? yin4.z : u == 2 ? yin4.y : yin4.x;
-        if constexpr (FWD && FUSE) {
-          v_in = vin4[u];
-        } else if constexpr (FWD) {
-          v_in = S.rin[p_slot][p_sub][jl][el];
-          if (++p_sub == WG) {
-            p_sub = 0;
-            p_slot = p_slot + 1 == WPG ? 0 : p_slot + 1;
+        for (int u = 0; u < WG; u++) {
+          const int t = gi * WG + u;
+          const int uc = h * WG + u;  // step within the chunk
+          const float *yprev = &S.y[(t + 1) & 1][0][0];  // values of step t-1
+          const float k0 = u == 0 ? c0.x : u == 1 ? c0.y : u == 2 ? c0.z : c0.w;
+          const float k1 = u == 0 ? c1.x : u == 1 ? c1.y : u == 2 ? c1.z : c1.w;
+          const float k2 = u == 0 ? c2.x : u == 1 ? c2.y : u == 2 ? c2.z : c2.w;
+          const float k3 = u == 0 ? c3.x : u == 1 ? c3.y : u == 2 ? c3.z : c3.w;
+          // backward y: forward step nsteps-1-t, component 3-u of the group
+          float v_in = u == 0 ? yin4.w : u == 1 ? yin4.z : u == 2 ? yin4.y : yin4.x;
+          if constexpr (FWD && FUSE) {
+            v_in = vin4[u];
+          } else if constexpr (FWD) {
+            v_in = S.rin[p_slot][p_sub][jl][el];
+            if (++p_sub == WG) {
+              p_sub = 0;
+              p_slot = p_slot + 1 == WPG ? 0 : p_slot + 1;
+            }
+          }
+          // Branch-free step: a coupling the point does not have is applied as
+          // the product of a zero coefficient (the streams hold zeros there) and
+          // a finite operand (the neighbour value is zeroed by a select), which
+          // subtracts an exact zero; the terms keep lusol's order, so the
+          // values are lusol's (an exact-zero result may differ in its sign
+          // only).  With no branches the scheduler overlaps the point's own
+          // terms with the neighbour loads that follow the barrier.
+          const int q = t - shift - sk;
+          const bool act = INNER ? valid : valid && (unsigned)q < (unsigned)npm2;
+          const int kk = FWD ? q : npm2 - 1 - q;
+          const float *pe = ext_e ? ring + ring_e + uc * 16 : yprev + y_e;
+          const float *pj = ext_j ? ring + ring_j + uc * 16 : yprev + y_j;
+          const float ne = cpl_e ? *pe : 0.f;
+          const float nj = cpl_j ? *pj : 0.f;
+          float y;
+          if constexpr (FWD) {
+            // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1); l_k = 0 on the first plane
+            if constexpr (INNER) {
+              y = __fsub_rn(v_in, __fmul_rn(k0, prev));
+            } else {
+              const float ks = kk == npm2 - 1 ? seam_c : 0.f;
+              y = __fsub_rn(__fsub_rn(v_in, __fmul_rn(ks, seam_y)), __fmul_rn(k0, prev));
+            }
+            y = __fsub_rn(y, __fmul_rn(k1, nj));
+            y = __fsub_rn(y, __fmul_rn(k2, ne));
+            y = act ? y : 0.f;
+            if constexpr (!INNER) seam_y = (act && kk == 0) ? y : seam_y;
+            rn4[u] = act ? v_in : 0.f;
+          } else {
+            // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv; u_k = 0 on the last plane
+            y = __fsub_rn(v_in, __fmul_rn(k0, ne));
+            y = __fsub_rn(y, __fmul_rn(k1, nj));
+            y = __fsub_rn(y, __fmul_rn(k2, prev));
+            if constexpr (!INNER) {
+              const float ks = kk == 0 ? seam_c : 0.f;
+              y = __fsub_rn(y, __fmul_rn(ks, seam_y));
+            }
+            y = __fmul_rn(y, k3);
+            y = act ? y : 0.f;
+            if constexpr (!INNER) seam_y = (act && kk == npm2 - 1) ? y : seam_y;
+            if (act) S.zout[kk % WROUT][T] = y;
+            if constexpr (FUSE) {
+              // the point's r32 (forward step nsteps-1-t, component 3-u, as
+              // for y); r and z are exact zeros where the thread has no point
+              const float rr = u == 0 ? r_cur.w : u == 1 ? r_cur.z : u == 2 ? r_cur.y : r_cur.x;
+              rz = fma((double)rr, (double)y, rz);
+            }
+          }
+          S.y[t & 1][jl][el] = y;
+          if (pub_e && act) wave_publish(xe_out + (size_t)t * 16, epoch, y);
+          if (pub_j && act) wave_publish(xj_out + (size_t)t * 16, epoch, y);
+          prev = INNER ? y : act ? y : prev;  // inner: y is already 0 where the thread has no point
+          y4[u] = y;
+          // backward: the group's z32 plane writes become visible to the copy
+          // warp's TMA stores (async proxy) across the barrier and gdone
+          if (!FWD && u == WG - 1) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          if (u == WG - 1) {
+            // the group's last barrier also ORs the abort flag, so every compute
+            // warp leaves at the same group when any wait gave up
+            aborted = wave_bar_compute_any(*(volatile int *)&S.abort != 0);
+          } else {
+            wave_bar_compute();
           }
         }
-        // Branch-free step: a coupling the point does not have is applied as
-        // the product of a zero coefficient (the streams hold zeros there) and
-        // a finite operand (the neighbour value is zeroed by a select), which
-        // subtracts an exact zero; the terms keep lusol's order, so the
-        // values are lusol's (an exact-zero result may differ in its sign
-        // only).  With no branches the scheduler overlaps the point's own
-        // terms with the neighbour loads that follow the barrier.
-        const int q = t - shift - sk;
-        const bool act = valid && (unsigned)q < (unsigned)npm2;
-        const int kk = FWD ? q : npm2 - 1 - q;
-        const float *pe = ext_e ? ring + ring_e + uc * 16 : yprev + y_e;
-        const float *pj = ext_j ? ring + ring_j + uc * 16 : yprev + y_j;
-        const float ne = cpl_e ? *pe : 0.f;
-        const float nj = cpl_j ? *pj : 0.f;
-        float y;
-        if constexpr (FWD) {
-          // y = r - [seam] - l_k y(k-1) - l_j y(j-1) - l_e y(e-1); l_k = 0 on the first plane
-          const float ks = kk == npm2 - 1 ? seam_c : 0.f;
-          y = __fsub_rn(__fsub_rn(v_in, __fmul_rn(ks, seam_y)), __fmul_rn(k0, prev));
-          y = __fsub_rn(y, __fmul_rn(k1, nj));
-          y = __fsub_rn(y, __fmul_rn(k2, ne));
-          y = act ? y : 0.f;
-          seam_y = (act && kk == 0) ? y : seam_y;
-          rn4[u] = act ? v_in : 0.f;
-        } else {
-          // z = (y - u_e z(e+1) - u_j z(j+1) - u_k z(k+1) - [seam]) * dinv; u_k = 0 on the last plane
-          const float ks = kk == 0 ? seam_c : 0.f;
-          y = __fsub_rn(v_in, __fmul_rn(k0, ne));
-          y = __fsub_rn(y, __fmul_rn(k1, nj));
-          y = __fsub_rn(y, __fmul_rn(k2, prev));
-          y = __fsub_rn(y, __fmul_rn(ks, seam_y));
-          y = __fmul_rn(y, k3);
-          y = act ? y : 0.f;
-          seam_y = (act && kk == npm2 - 1) ? y : seam_y;
-          if (act) S.zout[kk % WROUT][T] = y;
-          if constexpr (FUSE) {
-            // the point's r32 (forward step nsteps-1-t, component 3-u, as
-            // for y); r and z are exact zeros where the thread has no point
-            const float rr = u == 0 ? r_cur.w : u == 1 ? r_cur.z : u == 2 ? r_cur.y : r_cur.x;
-            rz = fma((double)rr, (double)y, rz);
-          }
-        }
-        S.y[t & 1][jl][el] = y;
-        if (pub_e && act) wave_publish(xe_out + (size_t)t * 16, epoch, y);
-        if (pub_j && act) wave_publish(xj_out + (size_t)t * 16, epoch, y);
-        prev = act ? y : prev;
-        y4[u] = y;
-        // backward: the group's z32 plane writes become visible to the copy
-        // warp's TMA stores (async proxy) across the barrier and gdone
-        if (!FWD && u == WG - 1) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (u == WG - 1) {
-          // the group's last barrier also ORs the abort flag, so every compute
-          // warp leaves at the same group when any wait gave up
-          if (wave_bar_compute_any(*(volatile int *)&S.abort != 0)) return false;
-        } else {
-          wave_bar_compute();
-        }
-      }
+        return aborted;
+      };
+      // inner: 1 <= q <= npm2 - 2 for every thread (0 <= sk <= WSK) at every step of the group
+      const bool inner = WG * gi >= shift + WSK + 1 && WG * gi + (WG - 1) <= shift + npm2 - 2;
+      if (inner ? steps(std::true_type{}) : steps(std::false_type{})) return false;
       if constexpr (FWD) a.ys[((size_t)ti * G + gi) * WAVE_THREADS + T] = make_float4(y4[0], y4[1], y4[2], y4[3]);
       if constexpr (FWD && FUSE)
         a.rs[((size_t)ti * G + gi) * WAVE_THREADS + T] = make_float4(rn4[0], rn4[1], rn4[2], rn4[3]);
