@@ -530,13 +530,17 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
   float4 r_cur = make_float4(0.f, 0.f, 0.f, 0.f), r_next = r_cur;
   if constexpr (FUSE && !FWD) r_next = a.rs[((size_t)ti * G + (G - 1)) * WAVE_THREADS + T];
   // forward: plane p = t - sk of this line sits in slot (qbase + p / WG) % WPG,
-  // row p % WG (p < 0 at the first steps: the entry is never read)
-  int p_sub = 0, p_slot = 0;
-  {
+  // row p % WG (p < 0 at the first steps: the entry is never read); the slots
+  // are consecutive in shared memory, so the plane's place is one index
+  // p_lin = slot * WG + row into a ring of WPG * WG planes
+  constexpr int NPL = WPG * WG;
+  const float *rin_line = nullptr;  // + p_lin * WJT * WE
+  int p_lin = 0;
+  if constexpr (FWD) {
+    rin_line = &S.rin[0][0][jl][el];
     const int p0 = -sk;  // plane at step 0
     const int pg = (p0 - (WG - 1)) / WG;  // floor(p0 / WG) for p0 <= 0
-    p_sub = p0 - pg * WG;
-    p_slot = ((qbase + pg) % WPG + WPG) % WPG;
+    p_lin = (((qbase + pg) % WPG + WPG) % WPG) * WG + (p0 - pg * WG);
   }
 #pragma unroll 1
   for (int c = 0; c < nch; c++) {
@@ -600,14 +604,12 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
         // every plane of the group's steps arrived with group gi's copies
 #pragma unroll
         for (int u = 0; u < WG; u++) {
-          const float qv = S.rin[p_slot][p_sub][jl][el];
-          if (++p_sub == WG) {
-            p_sub = 0;
-            p_slot = p_slot + 1 == WPG ? 0 : p_slot + 1;
-          }
+          const int pl = p_lin + u < NPL ? p_lin + u : p_lin + u - NPL;
+          const float qv = rin_line[pl * (WJT * WE)];
           const float ro = u == 0 ? c3.x : u == 1 ? c3.y : u == 2 ? c3.z : c3.w;
           vin4[u] = (float)fma(-alpha, (double)qv, (double)ro);  // r32 - alpha q
         }
+        p_lin = p_lin + WG < NPL ? p_lin + WG : p_lin + WG - NPL;
       }
       // The group's steps, in two compiled forms.  INNER: every thread's
       // plane is strictly inside its line at all four steps (neither the
@@ -620,6 +622,9 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
       auto steps = [&](auto inner_tag) -> bool {
         constexpr bool INNER = decltype(inner_tag)::value;
         bool aborted = false;
+        // backward, inner: plane kk of step u sits in zout slot kk % WROUT, counted down from the group's first
+        int zs0 = 0;
+        if constexpr (!FWD && INNER) zs0 = (npm2 - 1 - (gi * WG - shift - sk)) % WROUT;
 #pragma unroll
         for (int u = 0; u < WG; u++) {
           const int t = gi * WG + u;
@@ -634,11 +639,8 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
           if constexpr (FWD && FUSE) {
             v_in = vin4[u];
           } else if constexpr (FWD) {
-            v_in = S.rin[p_slot][p_sub][jl][el];
-            if (++p_sub == WG) {
-              p_sub = 0;
-              p_slot = p_slot + 1 == WPG ? 0 : p_slot + 1;
-            }
+            v_in = rin_line[p_lin * (WJT * WE)];
+            p_lin = p_lin + 1 < NPL ? p_lin + 1 : 0;
           }
           // Branch-free step: a coupling the point does not have is applied as
           // the product of a zero coefficient (the streams hold zeros there) and
@@ -680,7 +682,12 @@ __device__ __forceinline__ bool wave_tile(const WaveArgs &a,
             y = __fmul_rn(y, k3);
             y = act ? y : 0.f;
             if constexpr (!INNER) seam_y = (act && kk == npm2 - 1) ? y : seam_y;
-            if (act) S.zout[kk % WROUT][T] = y;
+            if constexpr (INNER) {
+              const int zs = zs0 - u >= 0 ? zs0 - u : zs0 - u + WROUT;
+              if (act) S.zout[zs][T] = y;
+            } else {
+              if (act) S.zout[kk % WROUT][T] = y;
+            }
             if constexpr (FUSE) {
               // the point's r32 (forward step nsteps-1-t, component 3-u, as
               // for y); r and z are exact zeros where the thread has no point
