@@ -686,7 +686,7 @@ __global__ void k_cast_r32(long long n, const double *__restrict__ r, float *__r
 // in iteration order, so x is bit-identical to updating it every iteration,
 // and the solution vector is read and written once per group.  Four
 // unknowns per thread and pass.  Batches use pairs; a single solve groups
-// four (k_update_x_quad).
+// eight (k_update_x_oct).
 __device__ __forceinline__ void x_pair_body(const Geo &g, const SolveState *st, double *__restrict__ x,
                                             const float *__restrict__ pa, const float *__restrict__ pb, long long t0,
                                             long long stride) {
@@ -715,28 +715,34 @@ __device__ __forceinline__ void x_pair_body(const Geo &g, const SolveState *st, 
     *reinterpret_cast<double2 *>(x + id + 2) = x1;
   }
 }
-// The single solve's groups: four iterations at once, x += a_0 p_0 + a_1 p_1 +
-// a_2 p_2 + a_3 p_3 in iteration order (the directions of four consecutive
-// iterations, in the four rotating buffers), 8 B per unknown and iteration.
-__global__ void __launch_bounds__(NTHR) k_update_x_quad(Geo g, const SolveState *st, double *__restrict__ x,
-                                                        const float *__restrict__ p0, const float *__restrict__ p1,
-                                                        const float *__restrict__ p2, const float *__restrict__ p3) {
-  double a[4];
+// The single solve's groups: eight iterations at once, x += a_0 p_0 + ... +
+// a_7 p_7 in iteration order (the directions of eight consecutive
+// iterations, in the eight rotating buffers), x read and written once per
+// eight iterations: 6 B per unknown and iteration.
+struct XDirs {
+  const float *p[X_GROUP];
+};
+__global__ void __launch_bounds__(NTHR) k_update_x_oct(Geo g, const SolveState *st, double *__restrict__ x,
+                                                       XDirs d) {
+  double a[X_GROUP];
+  bool any = false;
 #pragma unroll
-  for (int i = 0; i < 4; i++) a[i] = *(const volatile double *)&st->xa[i];
-  if (a[0] == 0.0 && a[1] == 0.0 && a[2] == 0.0 && a[3] == 0.0) return;
-  const float *p[4] = {p0, p1, p2, p3};
+  for (int i = 0; i < X_GROUP; i++) {
+    a[i] = *(const volatile double *)&st->xa[i];
+    any = any || a[i] != 0.0;
+  }
+  if (!any) return;
   const long long n4 = g.Np / 4;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4;
        t += (long long)gridDim.x * blockDim.x) {
     const long long id = 4 * t;
     double2 x0 = *reinterpret_cast<const double2 *>(x + id);
     double2 x1 = *reinterpret_cast<const double2 *>(x + id + 2);
-    float4 v[4];
+    float4 v[X_GROUP];
 #pragma unroll
-    for (int i = 0; i < 4; i++) v[i] = __ldg(reinterpret_cast<const float4 *>(p[i] + id));
+    for (int i = 0; i < X_GROUP; i++) v[i] = __ldg(reinterpret_cast<const float4 *>(d.p[i] + id));
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < X_GROUP; i++) {
       if (a[i] != 0.0) {
         x0.x = fma(a[i], (double)v[i].x, x0.x);
         x0.y = fma(a[i], (double)v[i].y, x0.y);
@@ -1323,7 +1329,8 @@ int Solver::setup(const pot3d_mesh_t *mesh, const double *br0, const double *br1
     if (ifprec == 2) {
       m_p32q[0] = m_p32a;
       m_p32q[1] = m_p32b;
-      if ((st = alloc((void **)&m_p32q[2], fb)) || (st = alloc((void **)&m_p32q[3], fb))) return st;
+      for (int i = 2; i < X_GROUP; i++)
+        if ((st = alloc((void **)&m_p32q[i], fb))) return st;
     }
     if (ifprec != 2 && (st = alloc((void **)&m_r32, fb))) return st;  // ILU(0) uses the sweeps' r32
     CK(cudaEventCreate(&evm0));
@@ -1718,8 +1725,8 @@ int Solver::launch_iteration32(int u) {
   dim3 grid(g.nit, g.njt, g.nkc);
   dim3 gridu(g.nit, g.njt, g.nkc_u);
   if (ifprec == 2) {  // the rotation of four directions: position u reads buffer u % 4, writes the next
-    p32_cur = m_p32q[u & 3];
-    p32_nxt = m_p32q[(u + 1) & 3];
+    p32_cur = m_p32q[u % X_GROUP];
+    p32_nxt = m_p32q[(u + 1) % X_GROUP];
   }
   StencilArgs sa{};
   sa.p_new32 = p32_nxt;
@@ -1744,13 +1751,16 @@ int Solver::launch_iteration32(int u) {
   if (ifprec == 2) {
     if ((stm = tensor_map(dilu_z32(this), false, &mp.m32[1]))) return stm;
     mp.m32[2] = mp.m32[0];
-    sa.xslot1 = 1 + (u & 3);
+    sa.xslot1 = 1 + u % X_GROUP;
     k_stencil<MODE_PCGZ32><<<grid, NTHR, StageLayout<MODE_PCGZ32>::smem, stream>>>(mp, g, m, sa);
-    // after every fourth iteration x += the four iterations' alpha p (their
-    // directions are buffers 1, 2, 3, 0); the sweeps with r32 -= alpha q,
-    // rho, beta and ernorm inside them; the south-ring sums of z
-    if ((u & 3) == 3)
-      k_update_x_quad<<<xblocks, NTHR, 0, stream>>>(g, d_state, d_x, m_p32q[1], m_p32q[2], m_p32q[3], m_p32q[0]);
+    // after every eighth iteration x += the eight iterations' alpha p (the
+    // direction of iteration slot i is buffer i + 1 mod 8); the sweeps with
+    // r32 -= alpha q, rho, beta and ernorm inside them; the south-ring sums of z
+    if (u % X_GROUP == X_GROUP - 1) {
+      XDirs dirs;
+      for (int i = 0; i < X_GROUP; i++) dirs.p[i] = m_p32q[(i + 1) % X_GROUP];
+      k_update_x_oct<<<xblocks, NTHR, 0, stream>>>(g, d_state, d_x, dirs);
+    }
     int st = dilu_sweeps_fused(this, m_q32);
     if (st) return st;
     k_south_ring_z<<<dim3((g.nrm2 + 127) / 128, g.nkc_u), 128, 0, stream>>>(g, m, dilu_z32(this), d_s1z);
@@ -1880,13 +1890,14 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   const double est_iter_s = (ilu ? 100.0 : 60.0) * (double)g.Np / 5.0e12 + 6e-6;
   int U = (int)std::ceil(2.0e-3 / est_iter_s);
   U = std::max(1, std::min(U, 8));
-  if (ilu) U = (U + 1) & ~1;  // whole groups of four iterations (the rotation and the x update)
+  if (ilu) U = (U + X_GROUP / 2 - 1) / (X_GROUP / 2) * (X_GROUP / 2);  // whole groups of eight iterations
+                                                                        // (the rotation and the x update)
   if (!graph32_exec || graph32_U != U) {
     if (graph32_exec) cudaGraphExecDestroy(graph32_exec);
     graph32_exec = nullptr;
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    for (int u = 0; u < 2 * U; u++) {  // even count (ILU(0): multiple of 4): the directions return to m_p32a
+    for (int u = 0; u < 2 * U; u++) {  // even count (ILU(0): multiple of 8): the directions return to m_p32a
       st = launch_iteration32(u);
       if (st) {
         cudaStreamEndCapture(stream, &graph);
@@ -1902,9 +1913,9 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
   }
   const long long per_graph = 2LL * U;
   // kernels per iteration (ILU(0): stencil, sweeps, ring sums; plus one x
-  // update per four iterations)
+  // update per eight iterations)
   const long long nodes_per_iter = ilu ? 2 + sweep_launches() : 2;
-  const long long extra_per_graph = ilu ? U / 2 : 0;
+  const long long extra_per_graph = ilu ? 2LL * U / X_GROUP : 0;
   double rho_ref = h_state->rho;  // r.z at the last FP64 residual
   int ncg_ref = 0;                // iterations at the last FP64 residual
   int n_refine = 0, stagnant = 0, stalls = 0;
@@ -1937,10 +1948,11 @@ int Solver::mixed_solve(bool zero_guess, int ncgmax, double epscg, int *ierr, po
     CK(cudaMemcpyAsync(h_state, d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     if (h_state->status != ST_RUNNING) break;
-    if (ilu && (ran & 3)) {
-      // the graph stopped inside a group of four: the newest p is in buffer
-      // ran % 4, the next graph's first iteration reads buffer 0
-      CK(cudaMemcpyAsync(m_p32q[0], m_p32q[ran & 3], sizeof(float) * g.Np, cudaMemcpyDeviceToDevice, stream));
+    if (ilu && (ran % X_GROUP)) {
+      // the graph stopped inside a group of eight: the newest p is in buffer
+      // ran % 8, the next graph's first iteration reads buffer 0
+      CK(cudaMemcpyAsync(m_p32q[0], m_p32q[ran % X_GROUP], sizeof(float) * g.Np, cudaMemcpyDeviceToDevice,
+                         stream));
     } else if (!ilu && (ran & 1)) {
       // the graph stopped after an odd number of iterations: the newest p is
       // in the buffer the next graph writes first

@@ -21,6 +21,7 @@ namespace pot3d {
 constexpr int TI = 64;      // radial points per tile (32 lanes x 2)
 constexpr int TJ = 8;       // theta rows per tile (one warp each)
 constexpr int NTHR = 256;   // threads per tile block
+constexpr int X_GROUP = 8;  // refined ILU(0) single solve: iterations per solution update
 constexpr int SROW = TI + 4;  // shared-memory row: [pad, halo-, 64 own, halo+, pad]
 
 // Mesh arrays on the device, 1-based Fortran indexing: arr[k] is Fortran
@@ -55,7 +56,7 @@ struct Geo {
 struct SolveState {
   double rho, rho_old, alpha, beta, bdotb, epsn, pq, epscg;
   double rho_true;  // refined mode: preconditioned FP64 residual norm^2
-  double xa[4];     // refined ILU(0): alphas of the x updates applied in groups (0: none)
+  double xa[X_GROUP];  // refined ILU(0): alphas of the x updates applied in groups (0: none)
   int ncg, ncgmax, status, par;
   unsigned int cnt_a, cnt_b, cnt_c, pad0;
   int hist_cap, n_refine, inner, pad1;

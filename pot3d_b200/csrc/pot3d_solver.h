@@ -44,7 +44,7 @@ struct Solver {
   float *m_p32a = nullptr, *m_p32b = nullptr, *m_r32 = nullptr, *m_q32 = nullptr;
   // ILU(0): four directions in rotation (a, b and two more), so the solution
   // update is applied once per four iterations
-  float *m_p32q[4] = {nullptr, nullptr, nullptr, nullptr};
+  float *m_p32q[X_GROUP] = {};  // refined ILU(0): the directions of X_GROUP consecutive iterations
   float *p32_cur = nullptr, *p32_nxt = nullptr;
   cudaGraphExec_t graph32_exec = nullptr;
   int graph32_U = 0;
